@@ -1,0 +1,242 @@
+/*
+ * spt.h -- C-ABI of the B200 (sm_100a) path-tracing backend.
+ *
+ * This is the drop-in boundary: the reference renderer's C++ interfaces
+ * (AccelStructure, Integrator, BSDF/LayeredBSDF/Material, Camera, PixelSampler,
+ * ImageBuffer) are served by the entry points below.  Every signature uses plain
+ * pointers, sizes and POD structs; no C++ or torch types cross it, and no C++
+ * exception crosses it (every entry point returns an spt_status).
+ *
+ * Conventions
+ *   - Host pointers unless the name ends in _device; *_device entry points take
+ *     device pointers and a cudaStream_t passed as void*, and return without
+ *     synchronising.
+ *   - Images are row-major [y][x] (row 0 = top), RGB triplets of float.  The
+ *     reference stores ImageBuffer pixels as [x][y] (core/image_buffer.h:51); only
+ *     the memory order differs, pixel (x, y) means the same pixel.
+ *   - Primitive ids are indices into spt_scene_desc's primitive list, in the order
+ *     the primitives were given (the reference's Scene::primitives_ order,
+ *     core/scene.h:87).  A miss is reported as SPT_MISS.
+ *   - Rays are 8 floats: origin xyz, pad, direction xyz, pad (two float4s).  Like
+ *     the reference's Ray (core/ray.h:6-19) they carry no t range: a hit is any
+ *     t > 0 (acceleration/sbvh.cpp:494-496).
+ */
+#ifndef SPT_H
+#define SPT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPT_ABI_VERSION 1u
+#define SPT_MISS 0xFFFFFFFFu
+
+typedef enum spt_status {
+    SPT_OK = 0,
+    SPT_ERR_INVALID_ARGUMENT = 1,
+    SPT_ERR_CUDA = 2,
+    SPT_ERR_OUT_OF_MEMORY = 3,
+    SPT_ERR_OVERFLOW = 4,      /* a queue or stack capacity was exceeded; results are incomplete */
+    SPT_ERR_TIMEOUT = 5,       /* a bounded device loop ran out of iterations */
+    SPT_ERR_UNSUPPORTED = 6,
+    SPT_ERR_INTERNAL = 7
+} spt_status;
+
+/* Primitive kinds (reference primitives/triangle.h, smooth_triangle.h, sphere.h). */
+enum { SPT_PRIM_TRIANGLE = 0, SPT_PRIM_SMOOTH_TRIANGLE = 1, SPT_PRIM_SPHERE = 2 };
+
+/* BSDF kinds (reference materials/lambertian.h, smooth_conductor.h, smooth_dielectric.h,
+ * cook_torrance.h) and their sampler choice (reference lua_core/bsdfs.lua:8, the
+ * "uniform"/"importance" field; core/swpathtracer_app.cpp:89-149 maps it to a sampler). */
+enum { SPT_BSDF_LAMBERTIAN = 0, SPT_BSDF_SMOOTH_CONDUCTOR = 1, SPT_BSDF_SMOOTH_DIELECTRIC = 2,
+       SPT_BSDF_COOK_TORRANCE = 3 };
+enum { SPT_SAMPLER_UNIFORM = 0, SPT_SAMPLER_IMPORTANCE = 1 };
+
+/* Acceleration structure kinds (reference acceleration/accel_structure.h:17). BVH_SAH and
+ * SBVH_SAH build the same tree: the spatial-split half of the reference is disabled. */
+enum { SPT_ACCEL_NONE = 0, SPT_ACCEL_BVH_SAH = 1, SPT_ACCEL_SBVH_SAH = 2 };
+
+/* Camera kinds (reference cameras/camera.h:14) and pixel samplers (pixel_samplers/pixel_sampler.h:8). */
+enum { SPT_CAMERA_PINHOLE = 0, SPT_CAMERA_ORTHOGRAPHIC = 1 };
+enum { SPT_PIXEL_UNIFORM = 0, SPT_PIXEL_REGULAR = 1, SPT_PIXEL_JITTERED = 2 };
+
+/* Ray-caster pixel values (reference integrators/normal_raycaster.h, depth_raycaster.h,
+ * int_test_count_raycaster.h). */
+enum { SPT_RAYCAST_NORMAL = 0, SPT_RAYCAST_DEPTH = 1, SPT_RAYCAST_COUNT = 2 };
+
+/* Path termination (reference integrators/pathtracer.h:13). */
+enum { SPT_TERMINATE_MAX_DEPTH = 0, SPT_TERMINATE_RUSSIAN_ROULETTE = 1 };
+
+/* One BSDF layer.  rgb: Lambertian kd, conductor / Cook-Torrance reflectance at normal
+ * incidence.  scalar: dielectric IOR, Cook-Torrance roughness (Beckmann m). */
+typedef struct spt_bsdf {
+    int32_t type;
+    int32_t sampler;
+    float rgb[3];
+    float scalar;
+} spt_bsdf;
+
+/* Material = layered BSDF + emission (reference materials/material.h:8-20). */
+typedef struct spt_material {
+    uint32_t layered_bsdf;
+    float emission[3];
+} spt_material;
+
+/* Scene description (reference core/scene.h:22-90 + the Lua records that fill it).
+ * prim_data: 9 floats per primitive -- triangle v0 v1 v2, or sphere centre xyz, radius,
+ * 5 unused.  prim_normals: 9 floats per primitive (n0 n1 n2, used by smooth triangles);
+ * may be NULL when no smooth triangle is present.  layered_offsets has n_layered + 1
+ * entries into layered_bsdf_ids (top layer first, reference materials/layered_bsdf.cpp:20-23). */
+typedef struct spt_scene_desc {
+    uint32_t n_prims;
+    const uint8_t* prim_type;
+    const float* prim_data;
+    const float* prim_normals;
+    const uint32_t* prim_material;
+    uint32_t n_bsdfs;
+    const spt_bsdf* bsdfs;
+    uint32_t n_layered;
+    const uint32_t* layered_offsets;
+    const uint32_t* layered_bsdf_ids;
+    uint32_t n_materials;
+    const spt_material* materials;
+    float background[3];
+    int32_t accel;
+} spt_scene_desc;
+
+/* Camera + image buffer (reference cameras/pinhole_camera.h, orthographic_camera.h,
+ * core/image_buffer.h).  fov_deg is the vertical field of view. */
+typedef struct spt_camera {
+    int32_t type;
+    float position[3];
+    float look_at[3];
+    float up[3];
+    float fov_deg;
+    float min_x, max_x, min_y, max_y;
+    uint32_t width, height;
+    uint32_t vp_top, vp_left, vp_width, vp_height;
+} spt_camera;
+
+/* Path tracer settings (reference integrators/pathtracer.h:15-17 + lua_core/integrators.lua).
+ * max_depth: hard cap on surface interactions in russian-roulette mode; 0 means the
+ * reference's cap of 1000 bounces (integrators/pathtracer.cpp:44-45).  seed keys the
+ * counter-based Philox-4x32-10 generator that replaces the reference's per-thread
+ * mt19937 (core/prng.h).  spp_offset shifts the sample index so progressive passes
+ * draw fresh numbers. */
+typedef struct spt_pt_params {
+    int32_t pixel_sampler;
+    uint32_t spp;
+    int32_t termination;
+    int32_t path_length;
+    int32_t max_depth;
+    uint32_t spp_offset;
+    uint64_t seed;
+} spt_pt_params;
+
+/* Closest hit of one ray (reference core/intersection_record.h:6-12).  prim_id is
+ * SPT_MISS on a miss; then t = +inf.  u, v: barycentrics for triangles, 0 for spheres. */
+typedef struct spt_hit {
+    float t;
+    uint32_t prim_id;
+    float u, v;
+} spt_hit;
+
+/* Per-image statistics of the ray casters / path tracer (reference integrators/integrator.h:47-54). */
+typedef struct spt_render_stats {
+    uint64_t int_tests;
+    uint64_t int_hits;
+    uint64_t min_tests_pp, max_tests_pp;
+    uint64_t min_hits_pp, max_hits_pp;
+    uint64_t paths;       /* camera paths traced */
+    uint64_t segments;    /* ray segments traced (extend launches' rays) */
+    double gpu_ms;        /* device time of the render, CUDA events */
+} spt_render_stats;
+
+/* Flattened binary SAH tree (reference acceleration/sbvh.cpp:58-421).  Nodes in depth-first,
+ * left-first order: node i's left child is i + 1.  For inner nodes right = index of the right
+ * child and count = 0; for leaves right = first index into ref_prim and count = number of
+ * references.  Boxes are the reference's node AABBs (children inflated by 1e-3,
+ * acceleration/sbvh.cpp:409-412). */
+typedef struct spt_bvh2_node {
+    float min[3];
+    uint32_t right;
+    float max[3];
+    uint32_t count;
+} spt_bvh2_node;
+
+typedef struct spt_bvh_stats {
+    uint64_t num_nodes, num_inner_nodes, num_leaf_nodes, tree_height;
+    uint64_t min_prims_leaf, max_prims_leaf, num_references, num_unreferenced;
+    double build_ms;
+} spt_bvh_stats;
+
+typedef struct spt_context spt_context;
+typedef struct spt_scene spt_scene;
+typedef struct spt_bvh spt_bvh;
+
+/* ---- library / context --------------------------------------------------------------- */
+uint32_t spt_abi_version(void);
+/* Creates a context on CUDA device `device` (Integrator/Scene owner; reference
+ * core/swpathtracer_app.cpp:29-37 plays this role on the CPU). */
+spt_status spt_create(int device, spt_context** out);
+spt_status spt_destroy(spt_context* ctx);
+/* Text of the last error on this context (never NULL). */
+const char* spt_last_error(const spt_context* ctx);
+
+/* ---- acceleration structure (reference acceleration/accel_structure.h:15-35) --------- */
+/* Host build of the reference's full-sweep SAH tree, node for node
+ * (acceleration/sbvh.cpp:12-37, 58-421); n_threads <= 0 uses all cores. */
+spt_status spt_bvh_build(const spt_scene_desc* desc, int n_threads, spt_bvh** out);
+spt_status spt_bvh_stats_get(const spt_bvh* bvh, spt_bvh_stats* out);   /* SBVH::getStatistics, sbvh.h:72 */
+/* Copies the flattened tree out; either array may be NULL to query sizes only. */
+spt_status spt_bvh_export(const spt_bvh* bvh, spt_bvh2_node* nodes, uint64_t* n_nodes,
+                          uint32_t* ref_prim, uint64_t* n_refs);
+spt_status spt_bvh_free(spt_bvh* bvh);
+
+/* ---- scene upload (reference core/scene.h:22-90) --------------------------------------- */
+/* Copies the scene to the device.  bvh may be NULL: the tree is then built here
+ * (Scene::buildAccelStructure, core/scene.cpp:79-81). */
+spt_status spt_scene_create(spt_context* ctx, const spt_scene_desc* desc, const spt_bvh* bvh,
+                            spt_scene** out);
+spt_status spt_scene_destroy(spt_scene* scene);
+/* Device bytes held by the scene (nodes, triangles, materials). */
+uint64_t spt_scene_device_bytes(const spt_scene* scene);
+
+/* ---- ray queries (reference AccelStructure::intersect, accel_structure.h:29-30) ------- */
+/* Closest hit for n rays.  tests/hits (may be NULL): the reference's per-ray
+ * num_intersection_tests / num_intersections (sbvh.cpp:478-510), which come from a
+ * separate exhaustive binary-tree pass. */
+spt_status spt_intersect(spt_context* ctx, const spt_scene* scene, const float* rays, uint64_t n,
+                         spt_hit* hits, uint32_t* tests, uint32_t* nhits);
+spt_status spt_intersect_device(spt_context* ctx, const spt_scene* scene, const float* d_rays,
+                                uint64_t n, spt_hit* d_hits, void* stream);
+spt_status spt_count_device(spt_context* ctx, const spt_scene* scene, const float* d_rays,
+                            uint64_t n, uint32_t* d_tests, uint32_t* d_hits, void* stream);
+
+/* ---- integrators (reference integrators/integrator.h:8-55) ----------------------------- */
+/* Ray casters, one ray per pixel centre (integrators/raycaster.h:62-99).  out_host layout:
+ * NORMAL float[h][w][3] (0 on a miss), DEPTH float[h][w] (-1 on a miss), COUNT int64[h][w]. */
+spt_status spt_raycast_image(spt_context* ctx, const spt_scene* scene, const spt_camera* cam,
+                             int32_t mode, void* out_host, spt_render_stats* stats);
+spt_status spt_raycast_image_device(spt_context* ctx, const spt_scene* scene, const spt_camera* cam,
+                                    int32_t mode, void* d_out, void* stream);
+/* Path tracer (integrators/pathtracer.cpp:12-147).  out_rgb_host: float[h][w][3], the mean
+ * radiance per pixel over spp samples (before the sRGB conversion of saveImageToFile);
+ * pixels outside the viewport are 0. */
+spt_status spt_pathtrace(spt_context* ctx, const spt_scene* scene, const spt_camera* cam,
+                         const spt_pt_params* params, float* out_rgb_host, spt_render_stats* stats);
+spt_status spt_pathtrace_device(spt_context* ctx, const spt_scene* scene, const spt_camera* cam,
+                                const spt_pt_params* params, float* d_out_rgb, spt_render_stats* stats);
+
+/* ---- image post-processing (reference core/image_buffer.cpp and the ray casters' saveImageToFile) */
+/* sRGB (pow 1/2.2 of the clamped value) + ASCII P3 PPM writer, core/image_buffer.cpp:22-47. */
+spt_status spt_write_ppm(const char* path, const float* rgb, uint32_t width, uint32_t height, int32_t to_srgb);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPT_H */
