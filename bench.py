@@ -1,0 +1,298 @@
+#!/usr/bin/env python
+"""Throughput of the ray/scene hot path on B200.
+
+Workload (one "step"): closest-hit queries for 2^24 incoherent rays (origins uniform in a cube of
+side 3, directions uniform on the sphere) against a displaced icosphere of 1,310,720 triangles
+(radius 1, value-noise displacement amplitude 0.05, 8 octaves), tree = the reference's SAH tree.
+Metric: Mrays/s, whole job.  Each rank traces its own 2^24 rays (weak scaling, no collective on
+the data path; ranks only meet for the barrier and the max-over-ranks of the device time).
+
+Beside the headline it reports the 1920x1080 primary-ray modes (normal / depth / hit count) and,
+on rank 0 with one GPU, the reference's own CPU traversal timed on this host's cores.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mrays/s & Mpaths/s at 1M tris; equal-time relMSE guided vs plain"
+WORKLOAD = ("closest-hit ray queries: 2^24 incoherent rays vs a 1,310,720-triangle displaced icosphere "
+            "(reference SAH tree), FP32")
+HBM_FALLBACK_GBS = 6650.0
+
+
+def args_():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--rays-log2", type=int, default=24)
+    p.add_argument("--subdiv", type=int, default=8)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extras", action="store_true", help="skip the primary-ray and path-tracing side metrics")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return HBM_FALLBACK_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.samples = []
+        self.gpu = gpu_index
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.p = None
+
+    def _read(self):
+        for line in self.p.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.samples.append(f)
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_scene(subdiv):
+    from swpathtracer_b200 import scenes
+    return scenes.displaced_mesh_scene(subdiv).build()
+
+
+def cpu_baseline(packed, rays_np, budget_rays):
+    """The reference's own SBVH::intersect (oracle/_ref) on this host's cores, over a bounded sample."""
+    sample = rays_np[:budget_rays]
+    cores = os.cpu_count() or 1
+    try:
+        from oracle.bindings import RefHarness
+        h = RefHarness()
+        kind = "reference"
+        rs = h.scene(packed, n_threads=cores)
+        r = rs.intersect(sample, n_threads=cores, want_normals=False)
+        secs = r["seconds"]
+    except FileNotFoundError:
+        from oracle.bindings import Oracle
+        kind = "port"
+        osc = Oracle().scene(packed)
+        t0 = time.perf_counter()
+        osc.intersect(sample, n_threads=cores, want_normals=False)
+        secs = time.perf_counter() - t0
+    return {"value": round(len(sample) / secs / 1e6, 4), "unit": "Mrays/s", "cores": cores, "kind": kind,
+            "sample": "%d of the step's incoherent rays, SBVH::intersect per ray, OpenMP over rays" % len(sample)}
+
+
+def run_reference(a):
+    """--impl reference: the reference's CPU path on the same workload (rank 0 only)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from swpathtracer_b200 import scenes
+    packed = build_scene(a.subdiv)
+    n_step = 1 << 20
+    rays = scenes.incoherent_rays(1 << a.rays_log2, seed=1)
+    cores = os.cpu_count() or 1
+    try:
+        from oracle.bindings import RefHarness
+        rs = RefHarness().scene(packed, n_threads=cores)
+        kind = "reference"
+        run = lambda s: rs.intersect(s, n_threads=cores, want_normals=False)["seconds"]
+    except FileNotFoundError:
+        from oracle.bindings import Oracle
+        osc = Oracle().scene(packed)
+        kind = "port"
+
+        def run(s):
+            t0 = time.perf_counter()
+            osc.intersect(s, n_threads=cores, want_normals=False)
+            return time.perf_counter() - t0
+    for w in range(a.warmup):
+        run(rays[(w * n_step) % len(rays):][:n_step])
+    total = 0.0
+    for k in range(a.steps):
+        total += run(rays[(k * n_step) % len(rays):][:n_step])
+    value = a.steps * n_step / total / 1e6
+    out = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s", "n_gpus": a.gpus,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(1000 * total / a.steps, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "rays_per_step": n_step, "tris": int(packed.n_prims)},
+           "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": cores, "kind": kind,
+                            "sample": "%d rays per step of the 2^24-ray set, SBVH::intersect per ray" % n_step},
+           "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    a = args_()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import swpathtracer_b200 as spt
+    from swpathtracer_b200 import abi, scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    packed = build_scene(a.subdiv)
+    bvh = spt.Bvh(packed)
+    dev = spt.Device(local)
+    gs = spt.GpuScene(dev, packed, bvh)
+    n = 1 << a.rays_log2
+    rays_np = scenes.incoherent_rays(n, seed=1 + rank)
+    d_rays = torch.from_numpy(rays_np).to("cuda")
+    d_hits = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+
+    # reference traversal counts on a sample of the same rays: the per-ray algorithmic work
+    ns = 1 << 20
+    t_tests = torch.empty(ns, dtype=torch.int32, device="cuda")
+    t_prim = torch.empty(ns, dtype=torch.int32, device="cuda")
+    gs.count_device(d_rays.data_ptr(), ns, None, t_tests.data_ptr(), None, t_prim.data_ptr())
+    torch.cuda.synchronize()
+    t_tri = float(t_prim.double().mean())
+    t_box = float(t_tests.double().mean()) - t_tri
+    bytes_per_ray = 24.0 * t_box + 36.0 * t_tri + 32.0 + 16.0
+
+    def step():
+        gs.intersect_device(d_rays.data_ptr(), n, d_hits.data_ptr(), 0)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(a.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    ms_step = ms / a.steps
+    value = world * n * a.steps / (ms / 1000.0) / 1e6
+
+    # end to end through the public C-ABI entry point with pinned host buffers
+    h_rays = torch.from_numpy(rays_np).pin_memory()
+    h_rays_np = h_rays.numpy()
+    h_hits = torch.empty((n, 4), dtype=torch.int32).pin_memory().numpy().view(abi.HIT_DTYPE).reshape(n)
+    gs.intersect(h_rays_np, out=h_hits)
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(a.steps, 5))
+    for _ in range(e2e_steps):
+        gs.intersect(h_rays_np, out=h_hits)
+    e2e = n * e2e_steps / (time.perf_counter() - t0) / 1e6
+    if world > 1:
+        t = torch.tensor([e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        e2e = float(t.item()) * world
+
+    hbm, peak_kind = peaks()
+    achieved = bytes_per_ray * n / (ms_step / 1000.0) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tr = json.load(f).get("k_intersect")
+        if tr:
+            traffic = tr["bytes_per_ray"] * n
+
+    out = {"metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "rays_per_step_per_gpu": n, "tris": int(packed.n_prims),
+                      "l2": "inputs larger than L2: 512 MB of rays streamed per step (scene 97 MB stays in L2)",
+                      "parallelism": "replicas" if world > 1 else "single GPU"},
+           "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                        "frac": round(achieved / hbm, 4), "traffic": traffic,
+                        "peak_source": peak_kind,
+                        "algorithmic_bytes_per_ray": round(bytes_per_ray, 2),
+                        "ref_box_tests_per_ray": round(t_box, 3), "ref_tri_tests_per_ray": round(t_tri, 3)},
+           "e2e": {"value": round(e2e, 3), "unit": "Mrays/s", "h2d_bytes_per_step": n * 32,
+                   "d2h_bytes_per_step": n * 16},
+           "gpu_launches": a.steps,
+           "clocks": clk}
+
+    if rank == 0 and not a.no_extras:
+        extras = {}
+        for name, mode in (("normal", abi.RAYCAST_NORMAL), ("depth", abi.RAYCAST_DEPTH), ("count", abi.RAYCAST_COUNT)):
+            cam = scenes.displaced_mesh_camera(1920, 1080)
+            elem = {abi.RAYCAST_NORMAL: 12, abi.RAYCAST_DEPTH: 4, abi.RAYCAST_COUNT: 8}[mode]
+            buf = torch.empty(1920 * 1080 * elem, dtype=torch.uint8, device="cuda")
+            for _ in range(3):
+                gs.raycast_device(cam, mode, buf.data_ptr())
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(10):
+                gs.raycast_device(cam, mode, buf.data_ptr())
+            e1.record()
+            torch.cuda.synchronize()
+            extras["primary_1920x1080_" + name + "_Mrays_s"] = round(1920 * 1080 * 10 / (e0.elapsed_time(e1) / 1e3) / 1e6, 2)
+        out["submetrics"] = extras
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(packed, rays_np, 1 << 22)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    gs.close()
+    dev.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -213,8 +213,12 @@ spt_status spt_intersect(spt_context* ctx, const spt_scene* scene, const float* 
                          spt_hit* hits, uint32_t* tests, uint32_t* nhits);
 spt_status spt_intersect_device(spt_context* ctx, const spt_scene* scene, const float* d_rays,
                                 uint64_t n, spt_hit* d_hits, void* stream);
+/* The reference's own traversal order (unordered, unpruned, depth first): per-ray test counts
+ * (box + primitive tests, and the primitive tests alone) and, when d_ref_hits is not NULL, the
+ * hit that traversal keeps.  Any output may be NULL. */
 spt_status spt_count_device(spt_context* ctx, const spt_scene* scene, const float* d_rays,
-                            uint64_t n, uint32_t* d_tests, uint32_t* d_hits, void* stream);
+                            uint64_t n, spt_hit* d_ref_hits, uint32_t* d_tests, uint32_t* d_hits,
+                            uint32_t* d_prim_tests, void* stream);
 
 /* ---- integrators (reference integrators/integrator.h:8-55) ----------------------------- */
 /* Ray casters, one ray per pixel centre (integrators/raycaster.h:62-99).  out_host layout:

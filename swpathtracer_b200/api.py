@@ -1,0 +1,155 @@
+"""Python face of the backend: thin objects over the C-ABI handles.
+
+Device            spt_context on one CUDA device
+Bvh               spt_bvh, the host-built reference SAH tree (SBVH::build / getStatistics)
+GpuScene          spt_scene: a scene resident in HBM, answering ray queries and rendering
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi, native
+
+
+class Device:
+    """A context on one CUDA device (its stream, events and scratch buffers)."""
+
+    def __init__(self, device=0):
+        self.lib = native.lib()
+        h = C.c_void_p()
+        native.check(self.lib.spt_create(device, C.byref(h)), None, "spt_create(%d)" % device)
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.spt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, status, what=""):
+        native.check(status, self.h, what)
+
+
+class Bvh:
+    """The reference's SAH tree built on the host (acceleration/sbvh.cpp:12-37)."""
+
+    def __init__(self, packed, n_threads=0):
+        self.lib = native.lib()
+        h = C.c_void_p()
+        native.check(self.lib.spt_bvh_build(packed.ref(), n_threads, C.byref(h)), None, "spt_bvh_build")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.spt_bvh_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def statistics(self):
+        s = abi.BvhStats()
+        native.check(self.lib.spt_bvh_stats_get(self.h, C.byref(s)))
+        return s
+
+    def export(self):
+        nn, nr = C.c_uint64(), C.c_uint64()
+        self.lib.spt_bvh_export(self.h, None, C.byref(nn), None, C.byref(nr))
+        nodes = np.zeros(nn.value, abi.BVH2_NODE_DTYPE)
+        refs = np.zeros(nr.value, np.uint32)
+        native.check(self.lib.spt_bvh_export(self.h, nodes.ctypes.data, C.byref(nn), refs.ctypes.data, C.byref(nr)))
+        return nodes, refs
+
+
+_MODE_OUT = {abi.RAYCAST_NORMAL: (np.float32, 3), abi.RAYCAST_DEPTH: (np.float32, 1), abi.RAYCAST_COUNT: (np.int64, 1)}
+
+
+class GpuScene:
+    """A scene uploaded to the device (Scene + its acceleration structure)."""
+
+    def __init__(self, device, packed, bvh=None):
+        self.dev = device
+        self.lib = device.lib
+        self.packed = packed
+        h = C.c_void_p()
+        device.check(self.lib.spt_scene_create(device.h, packed.ref(), bvh.h if bvh else None, C.byref(h)),
+                     "spt_scene_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.spt_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_bytes(self):
+        return self.lib.spt_scene_device_bytes(self.h)
+
+    # ---- ray queries -------------------------------------------------------------------------
+    def intersect(self, rays, counts=False, out=None):
+        """Closest hit per ray (rays: float32 [n, 8]); counts adds the reference's per-ray test counts.
+        out: optional preallocated (e.g. pinned) array of abi.HIT_DTYPE for the hits."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        hits = out if out is not None else np.zeros(n, abi.HIT_DTYPE)
+        assert hits.dtype == abi.HIT_DTYPE and hits.shape == (n,) and hits.flags["C_CONTIGUOUS"]
+        tests = np.zeros(n, np.uint32) if counts else None
+        nh = np.zeros(n, np.uint32) if counts else None
+        self.dev.check(self.lib.spt_intersect(self.dev.h, self.h, rays.ctypes.data, n, hits.ctypes.data,
+                                              None if tests is None else tests.ctypes.data,
+                                              None if nh is None else nh.ctypes.data), "spt_intersect")
+        return dict(hits=hits, tests=tests, nhits=nh)
+
+    def intersect_device(self, d_rays, n, d_hits, stream=0):
+        self.dev.check(self.lib.spt_intersect_device(self.dev.h, self.h, d_rays, n, d_hits, stream),
+                       "spt_intersect_device")
+
+    def count_device(self, d_rays, n, d_ref_hits, d_tests, d_hits, d_prim_tests=None, stream=0):
+        """The reference-order traversal: its hit (d_ref_hits) and per-ray test counts; any may be None."""
+        self.dev.check(self.lib.spt_count_device(self.dev.h, self.h, d_rays, n, d_ref_hits, d_tests, d_hits,
+                                                 d_prim_tests, stream), "spt_count_device")
+
+    # ---- integrators -------------------------------------------------------------------------
+    def raycast(self, cam, mode, stats=False):
+        dt, ch = _MODE_OUT[mode]
+        shape = (cam.height, cam.width, 3) if ch == 3 else (cam.height, cam.width)
+        out = np.zeros(shape, dt)
+        st = abi.RenderStats() if stats else None
+        self.dev.check(self.lib.spt_raycast_image(self.dev.h, self.h, C.byref(cam), mode, out.ctypes.data,
+                                                  C.byref(st) if st is not None else None), "spt_raycast_image")
+        return (out, st) if stats else out
+
+    def raycast_device(self, cam, mode, d_out, stream=0):
+        self.dev.check(self.lib.spt_raycast_image_device(self.dev.h, self.h, C.byref(cam), mode, d_out, stream),
+                       "spt_raycast_image_device")
+
+    def pathtrace(self, cam, params):
+        out = np.zeros((cam.height, cam.width, 3), np.float32)
+        st = abi.RenderStats()
+        self.dev.check(self.lib.spt_pathtrace(self.dev.h, self.h, C.byref(cam), C.byref(params), out.ctypes.data,
+                                              C.byref(st)), "spt_pathtrace")
+        return out, st
+
+    def pathtrace_device(self, cam, params, d_out):
+        st = abi.RenderStats()
+        self.dev.check(self.lib.spt_pathtrace_device(self.dev.h, self.h, C.byref(cam), C.byref(params), d_out,
+                                                     C.byref(st)), "spt_pathtrace_device")
+        return st
+
+
+def write_ppm(path, rgb, srgb=True):
+    """ImageBuffer::saveToFile (core/image_buffer.cpp:32-47), with convertTosRGB first when srgb."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w = rgb.shape[:2]
+    native.check(native.lib().spt_write_ppm(path.encode(), rgb.ctypes.data, w, h, 1 if srgb else 0), None,
+                 "spt_write_ppm")

@@ -1,0 +1,270 @@
+// raycast.cu -- batched ray queries and the three ray-cast integrators.
+//
+//   k_intersect   closest hit per ray (AccelStructure::intersect, accel_structure.h:29-30)
+//   k_count       the reference's exhaustive traversal: tests / passes per ray
+//   k_raycast     camera ray generation fused with the query and the pixel value of one
+//                 ray-caster mode (integrators/raycaster.h:62-99 + normal_raycaster.cpp:19-31,
+//                 depth_raycaster.cpp:36-48, int_test_count_raycaster.cpp:75-85)
+#include <cstring>
+#include <limits>
+
+#include "spt_internal.h"
+#include "traverse.cuh"
+
+namespace spt {
+namespace {
+
+constexpr int kBlock = 128;
+
+__global__ void __launch_bounds__(kBlock) k_intersect(DevScene S, const float4* __restrict__ rays, uint64_t n,
+                                                      spt_hit* __restrict__ hits, uint32_t* status) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+    Hit1 h = closest_hit<kStack>(S, f3v(a), f3v(b), status);
+    spt_hit o;
+    o.t = h.t;
+    o.prim_id = h.found ? slot_prim(S, h.slot) : SPT_MISS;
+    o.u = h.u;
+    o.v = h.v;
+    hits[i] = o;
+}
+
+__global__ void __launch_bounds__(kBlock) k_count(DevScene S, const float4* __restrict__ rays, uint64_t n,
+                                                  spt_hit* __restrict__ ref_hits, uint32_t* __restrict__ tests,
+                                                  uint32_t* __restrict__ nhits, uint32_t* __restrict__ prim_tests,
+                                                  uint32_t* status) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+    CountOut c;
+    Hit1 h = count_traverse<kStack>(S, f3v(a), f3v(b), c, status);
+    if (ref_hits) {
+        spt_hit o;
+        o.t = h.t;
+        o.prim_id = h.found ? slot_prim(S, h.slot) : SPT_MISS;
+        o.u = h.u;
+        o.v = h.v;
+        ref_hits[i] = o;
+    }
+    if (tests) tests[i] = c.tests;
+    if (nhits) nhits[i] = c.hits;
+    if (prim_tests) prim_tests[i] = c.prim_tests;
+}
+
+// Per-image statistics of integrator.h:47-54, reduced per warp then once per warp to global.
+struct StatAcc {
+    unsigned long long sum_tests, sum_hits, min_tests, max_tests, min_hits, max_hits;
+};
+
+__device__ __forceinline__ void reduce_stats(StatAcc* g, bool valid, uint32_t tests, uint32_t hits) {
+    unsigned long long st = valid ? tests : 0ull, sh = valid ? hits : 0ull;
+    unsigned mnt = valid ? tests : 0xFFFFFFFFu, mxt = valid ? tests : 0u;
+    unsigned mnh = valid ? hits : 0xFFFFFFFFu, mxh = valid ? hits : 0u;
+    for (int o = 16; o > 0; o >>= 1) {
+        st += __shfl_xor_sync(0xFFFFFFFFu, st, o);
+        sh += __shfl_xor_sync(0xFFFFFFFFu, sh, o);
+    }
+    mnt = __reduce_min_sync(0xFFFFFFFFu, mnt);
+    mxt = __reduce_max_sync(0xFFFFFFFFu, mxt);
+    mnh = __reduce_min_sync(0xFFFFFFFFu, mnh);
+    mxh = __reduce_max_sync(0xFFFFFFFFu, mxh);
+    if ((threadIdx.x & 31) == 0 && mnt != 0xFFFFFFFFu) {
+        atomicAdd(&g->sum_tests, st);
+        atomicAdd(&g->sum_hits, sh);
+        atomicMin(&g->min_tests, static_cast<unsigned long long>(mnt));
+        atomicMax(&g->max_tests, static_cast<unsigned long long>(mxt));
+        atomicMin(&g->min_hits, static_cast<unsigned long long>(mnh));
+        atomicMax(&g->max_hits, static_cast<unsigned long long>(mxh));
+    }
+}
+
+// 256 threads cover a 16x16 pixel tile; each warp an 8x4 sub-tile, so neighbouring lanes trace
+// neighbouring pixels (coherent primary rays).
+__device__ __forceinline__ void tile_pixel(uint32_t& x, uint32_t& y) {
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    x = blockIdx.x * 16 + (w & 1) * 8 + (lane & 7);
+    y = blockIdx.y * 16 + (w >> 1) * 4 + (lane >> 3);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) k_raycast(DevScene S, DevCamera cam, void* __restrict__ out,
+                                                 StatAcc* stats, uint32_t* status) {
+    uint32_t x, y;
+    tile_pixel(x, y);
+    const bool valid = x < cam.width && y < cam.height;
+    uint32_t tests = 0, hits = 0;
+    if (valid) {
+        V3 o, d;
+        camera_ray(cam, static_cast<float>(x) + 0.5f, static_cast<float>(y) + 0.5f, o, d);
+        const uint64_t idx = static_cast<uint64_t>(y) * cam.width + x;
+        if (MODE == SPT_RAYCAST_COUNT || stats) {
+            CountOut c;
+            Hit1 h = count_traverse<kStack>(S, o, d, c, status);
+            tests = c.tests;
+            hits = c.hits;
+            if (MODE == SPT_RAYCAST_COUNT) {
+                static_cast<long long*>(out)[idx] = static_cast<long long>(c.tests);
+            } else if (MODE == SPT_RAYCAST_DEPTH) {
+                static_cast<float*>(out)[idx] = h.found ? h.t : -1.0f;
+            } else {
+                V3 nrm = v3(0.0f, 0.0f, 0.0f);
+                if (h.found) {
+                    const uint32_t prim = slot_prim(S, h.slot);
+                    nrm = hit_normal(S, prim, h.u, h.v, hit_pos(S.prim_type[prim] == SPT_PRIM_SPHERE, o, d, h.t));
+                }
+                float* q = static_cast<float*>(out) + 3 * idx;
+                q[0] = nrm.x; q[1] = nrm.y; q[2] = nrm.z;
+            }
+        } else {
+            Hit1 h = closest_hit<kStack>(S, o, d, status);
+            if (MODE == SPT_RAYCAST_DEPTH) {
+                static_cast<float*>(out)[idx] = h.found ? h.t : -1.0f;
+            } else {
+                V3 nrm = v3(0.0f, 0.0f, 0.0f);
+                if (h.found) {
+                    const uint32_t prim = slot_prim(S, h.slot);
+                    nrm = hit_normal(S, prim, h.u, h.v, hit_pos(S.prim_type[prim] == SPT_PRIM_SPHERE, o, d, h.t));
+                }
+                float* q = static_cast<float*>(out) + 3 * idx;
+                q[0] = nrm.x; q[1] = nrm.y; q[2] = nrm.z;
+            }
+        }
+    }
+    if (stats) reduce_stats(stats, valid, tests, hits);
+}
+
+inline unsigned blocks_for(uint64_t n, int block) { return static_cast<unsigned>((n + block - 1) / block); }
+
+}  // namespace
+
+spt_status launch_intersect(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
+                            cudaStream_t s) {
+    if (n == 0) return SPT_OK;
+    if (n > (1ull << 36)) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "too many rays in one call");
+    k_intersect<<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n, d_hits,
+                                                         ctx->d_status);
+    SPT_CUDA(ctx, cudaGetLastError());
+    return SPT_OK;
+}
+
+spt_status launch_count(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_ref_hits,
+                        uint32_t* d_tests, uint32_t* d_hits, uint32_t* d_prim_tests, cudaStream_t s) {
+    if (n == 0) return SPT_OK;
+    if (n > (1ull << 36)) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "too many rays in one call");
+    k_count<<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n, d_ref_hits,
+                                                     d_tests, d_hits, d_prim_tests, ctx->d_status);
+    SPT_CUDA(ctx, cudaGetLastError());
+    return SPT_OK;
+}
+
+static spt_status launch_raycast(spt_context* ctx, const spt_scene* sc, const DevCamera& cam, int32_t mode, void* d_out,
+                                 StatAcc* d_stats, cudaStream_t s) {
+    dim3 grid((cam.width + 15) / 16, (cam.height + 15) / 16);
+    if (mode == SPT_RAYCAST_NORMAL)
+        k_raycast<SPT_RAYCAST_NORMAL><<<grid, 256, 0, s>>>(sc->dev, cam, d_out, d_stats, ctx->d_status);
+    else if (mode == SPT_RAYCAST_DEPTH)
+        k_raycast<SPT_RAYCAST_DEPTH><<<grid, 256, 0, s>>>(sc->dev, cam, d_out, d_stats, ctx->d_status);
+    else
+        k_raycast<SPT_RAYCAST_COUNT><<<grid, 256, 0, s>>>(sc->dev, cam, d_out, d_stats, ctx->d_status);
+    SPT_CUDA(ctx, cudaGetLastError());
+    return SPT_OK;
+}
+
+}  // namespace spt
+
+using namespace spt;
+
+extern "C" {
+
+spt_status spt_intersect(spt_context* ctx, const spt_scene* sc, const float* rays, uint64_t n, spt_hit* hits,
+                         uint32_t* tests, uint32_t* nhits) {
+    if (!ctx || !sc || (n && (!rays || !hits))) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0) return SPT_OK;
+    SPT_CUDA(ctx, cudaSetDevice(ctx->device));
+    spt_status st;
+    void *d_rays, *d_hits, *d_tests = nullptr, *d_nh = nullptr;
+    if ((st = scratch(ctx, 0, n * 32, &d_rays)) != SPT_OK) return st;
+    if ((st = scratch(ctx, 1, n * sizeof(spt_hit), &d_hits)) != SPT_OK) return st;
+    if (tests && (st = scratch(ctx, 2, n * 4, &d_tests)) != SPT_OK) return st;
+    if (nhits && (st = scratch(ctx, 3, n * 4, &d_nh)) != SPT_OK) return st;
+    SPT_CUDA(ctx, cudaMemcpyAsync(d_rays, rays, n * 32, cudaMemcpyHostToDevice, ctx->stream));
+    if ((st = launch_intersect(ctx, sc, static_cast<float*>(d_rays), n, static_cast<spt_hit*>(d_hits), ctx->stream)) != SPT_OK)
+        return st;
+    if (tests || nhits)
+        if ((st = launch_count(ctx, sc, static_cast<float*>(d_rays), n, nullptr, static_cast<uint32_t*>(d_tests),
+                               static_cast<uint32_t*>(d_nh), nullptr, ctx->stream)) != SPT_OK)
+            return st;
+    SPT_CUDA(ctx, cudaMemcpyAsync(hits, d_hits, n * sizeof(spt_hit), cudaMemcpyDeviceToHost, ctx->stream));
+    if (tests) SPT_CUDA(ctx, cudaMemcpyAsync(tests, d_tests, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (nhits) SPT_CUDA(ctx, cudaMemcpyAsync(nhits, d_nh, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    return check_status(ctx);
+}
+
+spt_status spt_intersect_device(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n,
+                                spt_hit* d_hits, void* stream) {
+    if (!ctx || !sc || (n && (!d_rays || !d_hits))) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    return launch_intersect(ctx, sc, d_rays, n, d_hits, static_cast<cudaStream_t>(stream));
+}
+
+spt_status spt_count_device(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n,
+                            spt_hit* d_ref_hits, uint32_t* d_tests, uint32_t* d_hits, uint32_t* d_prim_tests,
+                            void* stream) {
+    if (!ctx || !sc || (n && !d_rays)) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    return launch_count(ctx, sc, d_rays, n, d_ref_hits, d_tests, d_hits, d_prim_tests, static_cast<cudaStream_t>(stream));
+}
+
+spt_status spt_raycast_image(spt_context* ctx, const spt_scene* sc, const spt_camera* cam, int32_t mode,
+                             void* out_host, spt_render_stats* stats) {
+    if (!ctx || !sc || !out_host) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (mode < SPT_RAYCAST_NORMAL || mode > SPT_RAYCAST_COUNT) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "unknown mode");
+    SPT_CUDA(ctx, cudaSetDevice(ctx->device));
+    DevCamera dc;
+    spt_status st = make_camera(ctx, cam, dc);
+    if (st != SPT_OK) return st;
+    const uint64_t npx = static_cast<uint64_t>(dc.width) * dc.height;
+    const size_t elem = mode == SPT_RAYCAST_NORMAL ? 12 : (mode == SPT_RAYCAST_DEPTH ? 4 : 8);
+    void *d_out, *d_stats = nullptr;
+    if ((st = scratch(ctx, 0, npx * elem, &d_out)) != SPT_OK) return st;
+    if (stats) {
+        if ((st = scratch(ctx, 4, sizeof(StatAcc), &d_stats)) != SPT_OK) return st;
+        StatAcc init{0, 0, std::numeric_limits<unsigned long long>::max(), 0,
+                     std::numeric_limits<unsigned long long>::max(), 0};
+        SPT_CUDA(ctx, cudaMemcpyAsync(d_stats, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    SPT_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    if ((st = launch_raycast(ctx, sc, dc, mode, d_out, static_cast<StatAcc*>(d_stats), ctx->stream)) != SPT_OK) return st;
+    SPT_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    SPT_CUDA(ctx, cudaMemcpyAsync(out_host, d_out, npx * elem, cudaMemcpyDeviceToHost, ctx->stream));
+    StatAcc acc{};
+    if (stats) SPT_CUDA(ctx, cudaMemcpyAsync(&acc, d_stats, sizeof(acc), cudaMemcpyDeviceToHost, ctx->stream));
+    st = check_status(ctx);
+    if (st != SPT_OK) return st;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->int_tests = acc.sum_tests;
+        stats->int_hits = acc.sum_hits;
+        stats->min_tests_pp = acc.min_tests;
+        stats->max_tests_pp = acc.max_tests;
+        stats->min_hits_pp = acc.min_hits;
+        stats->max_hits_pp = acc.max_hits;
+        stats->paths = npx;
+        stats->segments = npx;
+        float ms = 0.0f;
+        SPT_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        stats->gpu_ms = ms;
+    }
+    return SPT_OK;
+}
+
+spt_status spt_raycast_image_device(spt_context* ctx, const spt_scene* sc, const spt_camera* cam, int32_t mode,
+                                    void* d_out, void* stream) {
+    if (!ctx || !sc || !d_out) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (mode < SPT_RAYCAST_NORMAL || mode > SPT_RAYCAST_COUNT) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "unknown mode");
+    DevCamera dc;
+    spt_status st = make_camera(ctx, cam, dc);
+    if (st != SPT_OK) return st;
+    return launch_raycast(ctx, sc, dc, mode, d_out, nullptr, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,71 @@
+// spt_internal.h -- host-side objects behind the C-ABI handles.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/spt.h"
+#include "bvh_build.h"
+#include "spt_device.cuh"
+
+struct spt_bvh {
+    spt::HostBvh tree;
+};
+
+struct spt_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint32_t* d_status = nullptr;  // device error word: bit 0 stack overflow, bit 1 queue overflow, bit 2 timeout
+    std::string err;
+    // scratch buffers reused across calls (grown on demand)
+    void* scratch[8] = {};
+    size_t scratch_bytes[8] = {};
+    void* pinned = nullptr;
+    size_t pinned_bytes = 0;
+};
+
+struct spt_scene {
+    spt_context* ctx = nullptr;
+    spt::DevScene dev{};
+    std::vector<void*> allocations;
+    uint64_t bytes = 0;
+    uint32_t tree_height = 0;
+    uint32_t n_materials = 0;
+    bool any_emission = false;
+};
+
+namespace spt {
+
+// Status helpers: every entry point records a message and returns a status, never throws.
+spt_status fail(spt_context* ctx, spt_status s, const std::string& msg);
+spt_status cuda_fail(spt_context* ctx, cudaError_t e, const char* what);
+#define SPT_CUDA(ctx, call)                                          \
+    do {                                                             \
+        cudaError_t e_ = (call);                                     \
+        if (e_ != cudaSuccess) return spt::cuda_fail((ctx), e_, #call); \
+    } while (0)
+
+// Grows scratch slot `i` of the context to at least `bytes`.
+spt_status scratch(spt_context* ctx, int i, size_t bytes, void** out);
+spt_status pinned(spt_context* ctx, size_t bytes, void** out);
+
+// Reads the device status word and maps it to a status (resets it).
+spt_status check_status(spt_context* ctx);
+
+// Host computation of the camera constants (cameras/camera.cpp:3-11, pinhole_camera.cpp:3-12,
+// orthographic_camera.cpp:5-19).
+spt_status make_camera(spt_context* ctx, const spt_camera* cam, DevCamera& out);
+
+// Kernel launchers (raycast.cu)
+spt_status launch_intersect(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
+                            cudaStream_t s);
+spt_status launch_count(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_ref_hits,
+                        uint32_t* d_tests, uint32_t* d_hits, uint32_t* d_prim_tests, cudaStream_t s);
+
+constexpr int kStack = 64;
+
+}  // namespace spt

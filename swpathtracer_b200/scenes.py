@@ -389,6 +389,22 @@ def layered_box_camera(width=800, height=600):
     return box_camera(width, height, scale=3.0)
 
 
+def smooth_mesh_scene(subdivisions=4, seed=3):
+    """Displaced icosphere as SmoothTriangle primitives (per-vertex normals = normalised vertex
+    positions of the undisplaced sphere) plus one sphere, inside the open unit box: covers smooth
+    normals, spheres and triangles in one tree."""
+    sb = SceneBuilder(background=(0.2, 0.3, 0.4))
+    _box_into(sb, 1.0)
+    m = sb.material(sb.layered_bsdf(sb.cook_torrance(roughness=0.4, reflectance_at_normal_incidence=CONDUCTOR_F0)))
+    v, f = icosphere(subdivisions)
+    n = v.astype(np.float32)[f]
+    pos = (v * (1.0 + 0.05 * fbm(v, seed=seed))[:, None] * 0.25 + np.array([0.35, 0.3, 0.5]))
+    sb.triangles(pos.astype(np.float32)[f], m, normals=n)
+    glass = sb.material(sb.layered_bsdf(sb.smooth_dielectric(ior=1.5)))
+    sb.sphere((0.72, 0.18, 0.45), 0.17, glass)
+    return sb
+
+
 def furnace_scene(material="lambertian", reflectance=0.999):
     """White furnace (reference samples/furnace_test.lua): emissive sphere r=10, Le 0.5, around a unit
     sphere of the given material with reflectance 0.999."""
