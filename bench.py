@@ -283,6 +283,22 @@ def main():
             e1.record()
             torch.cuda.synchronize()
             extras["primary_1920x1080_" + name + "_Mrays_s"] = round(1920 * 1080 * 10 / (e0.elapsed_time(e1) / 1e3) / 1e6, 2)
+        # path tracing: the CPU-runnable box scene (20,492 tris, 256x256, 16 spp, max length 5) and the
+        # 1.3M-tri layered scene (800x600, russian roulette after 3, max depth 16), Mpaths/s
+        for key, sb, cam, prm in (
+                ("pt_box_256x256_16spp", scenes.box_scene(5), scenes.box_camera(256, 256),
+                 scenes.pt_params(spp=16, sampler="jittered", termination="max-length", path_length=5, seed=3)),
+                ("pt_layered_800x600_rr3_max16", scenes.layered_box_scene(a.subdiv), scenes.layered_box_camera(800, 600),
+                 scenes.pt_params(spp=16, sampler="jittered", termination="russian-roulette", path_length=3,
+                                  max_depth=16, seed=4))):
+            pgs = spt.GpuScene(dev, sb.build())
+            img = torch.empty(cam.width * cam.height * 3, dtype=torch.float32, device="cuda")
+            pgs.pathtrace_device(cam, prm, img.data_ptr())
+            st = pgs.pathtrace_device(cam, prm, img.data_ptr())
+            extras[key + "_Mpaths_s"] = round(st.paths / (st.gpu_ms / 1e3) / 1e6, 3)
+            extras[key + "_Mrays_s"] = round(st.segments / (st.gpu_ms / 1e3) / 1e6, 2)
+            extras[key + "_segments_per_path"] = round(st.segments / st.paths, 3)
+            pgs.close()
         out["submetrics"] = extras
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(packed, rays_np, 1 << 22)

@@ -94,10 +94,16 @@ def main():
         packed = mk().build()
         rs = H.scene(packed, n_threads=8)
         img, secs = rs.pathtrace(cam, params, n_threads=8)
+        # a second, independent render measures the noise floor of the comparison
+        params.seed += 1000
+        img2, _ = rs.pathtrace(cam, params, n_threads=8)
+        params.seed -= 1000
+        floor = float(np.mean((img2 - img) ** 2 / (img ** 2 + 1e-2)))
         np.savez_compressed(os.path.join(HERE, name + ".npz"), image=img)
         pt[name] = {"scene_sha256": scene_hash(packed), "spp": params.spp, "seconds": round(secs, 2),
                     "termination": params.termination, "path_length": params.path_length,
-                    "width": cam.width, "height": cam.height}
+                    "width": cam.width, "height": cam.height, "relmse_two_reference_renders": floor,
+                    "mean": float(img.mean())}
         print(name, secs, flush=True)
     meta["pathtrace"] = pt
     with open(os.path.join(HERE, "golden.json"), "w") as f:
