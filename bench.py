@@ -299,6 +299,21 @@ def main():
             extras[key + "_Mrays_s"] = round(st.segments / (st.gpu_ms / 1e3) / 1e6, 2)
             extras[key + "_segments_per_path"] = round(st.segments / st.paths, 3)
             pgs.close()
+        # batched uneven scenes: 64 seeded scenes (1k-500k tris, 128^2-1024^2, 64 spp) in one wavefront,
+        # settings from the autotuner (its trials are not timed)
+        batch = scenes.batched_scenes()
+        jobs = [(spt.GpuScene(dev, sb.build()), cam, prm) for sb, cam, prm, _ in batch]
+        bufs = [torch.empty(cam.width * cam.height * 3, dtype=torch.float32, device="cuda") for _, cam, _ in jobs]
+        tune = spt.autotune(dev, jobs, None)
+        st = spt.render_batch(dev, jobs, [b.data_ptr() for b in bufs], tune=tune)
+        paths = sum(s_.paths for s_ in st)
+        extras["batch64_Mpaths_s"] = round(paths / (st[0].gpu_ms / 1e3) / 1e6, 3)
+        extras["batch64_Mrays_s"] = round(st[0].segments / (st[0].gpu_ms / 1e3) / 1e6, 2)
+        extras["batch64_tune"] = {"capacity": tune.capacity, "shade_block": tune.shade_block,
+                                  "traversal": tune.traversal, "check_every": tune.check_every}
+        extras["batch64_paths"] = paths
+        for g_, _, _ in jobs:
+            g_.close()
         out["submetrics"] = extras
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(packed, rays_np, 1 << 22)

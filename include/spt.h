@@ -235,6 +235,84 @@ spt_status spt_pathtrace(spt_context* ctx, const spt_scene* scene, const spt_cam
 spt_status spt_pathtrace_device(spt_context* ctx, const spt_scene* scene, const spt_camera* cam,
                                 const spt_pt_params* params, float* d_out_rgb, spt_render_stats* stats);
 
+/* ---- batched rendering and tuning (no reference counterpart) ---------------------------------
+ * Many scenes of uneven size and resolution rendered by one wavefront: the camera paths of all jobs
+ * share one pool of path slots and the iterations are replayed from one CUDA graph.  Each job's image
+ * is what spt_pathtrace_device would produce for it alone (up to float-add order).  */
+typedef struct spt_tune {
+    uint32_t capacity;      /* path slots in the wavefront pool */
+    uint32_t extend_block;  /* threads per block of the non-persistent extend kernel */
+    uint32_t shade_block;   /* threads per block of the shade kernel */
+    int32_t traversal;      /* -1 scene default, 0 binary pair nodes, 1 8-wide, 2 8-wide + dynamic fetch */
+    uint32_t check_every;   /* wavefront iterations between host checks for completion */
+    uint32_t reserved[3];
+} spt_tune;
+
+typedef struct spt_batch_job {
+    const spt_scene* scene;
+    spt_camera camera;
+    spt_pt_params params;
+} spt_batch_job;
+
+spt_status spt_tune_default(spt_tune* out);
+/* d_images[i]: device float[h][w][3] of job i.  stats (may be NULL): one per job; paths is the job's,
+ * segments and gpu_ms are the whole batch's.  tune may be NULL (defaults). */
+spt_status spt_batch_pathtrace(spt_context* ctx, const spt_batch_job* jobs, uint32_t n_jobs, float* const* d_images,
+                               const spt_tune* tune, spt_render_stats* stats);
+/* Times short trial renders of the batch (a few samples per pixel) under candidate settings and
+ * returns the fastest.  cache_path (may be NULL): a text file of earlier results keyed by the
+ * device name and the batch's shape; a hit skips the trials. */
+spt_status spt_autotune(spt_context* ctx, const spt_batch_job* jobs, uint32_t n_jobs, const char* cache_path,
+                        spt_tune* out);
+
+/* ---- neural path guiding (no reference counterpart) -------------------------------------------
+ * A learned sampling distribution over directions, mixed with BSDF sampling by one-sample MIS:
+ * a multiresolution hash grid (16 levels x 2 features, 2^19 entries per level) encodes the position,
+ * a 4-hidden-layer ReLU MLP of width 64 (bf16 tensor-core GEMMs, fp32 accumulation) maps it with the
+ * normal and outgoing direction to 8 von Mises-Fisher lobes.  Trained online by Adam on the
+ * radiance the path tracer itself collects. */
+typedef struct spt_guide_config {
+    float box_min[3], box_max[3];  /* positions are normalised by this box (e.g. the scene bounds) */
+    float lr;                      /* Adam learning rate */
+    uint32_t batch;                /* training records per optimiser step */
+    uint32_t max_steps;            /* optimiser steps per guided render before the model is frozen */
+    float mix;                     /* probability of sampling the guiding distribution */
+    uint64_t seed;                 /* parameter initialisation */
+} spt_guide_config;
+
+/* One training record: a scattering event and the radiance it led to. */
+typedef struct spt_guide_record {
+    float pos[3], weight;          /* weight: the record's estimate of f*cos*Li/pdf (luminance) */
+    float normal[3], pad0;
+    float wo[3], pad1;             /* outgoing (towards the previous vertex), world space */
+    float wi[3], pad2;             /* sampled incident direction, world space */
+} spt_guide_record;
+
+typedef struct spt_guide spt_guide;
+
+spt_status spt_guide_create(spt_context* ctx, const spt_guide_config* cfg, spt_guide** out);
+spt_status spt_guide_destroy(spt_guide* guide);
+/* Master parameters (fp32): grid [16][2^19][2] and the MLP weights, layer by layer [out][in]
+ * (48->64, 64->64 x3, 64->48).  Either pointer may be NULL. */
+spt_status spt_guide_get_params(spt_guide* guide, float* grid, float* mlp);
+spt_status spt_guide_set_params(spt_guide* guide, const float* grid, const float* mlp);
+/* Mixture for n samples (host arrays): in 12 floats each (pos, 0, normal, 0, wo, 0 as float4s);
+ * out 40 floats each: 8 lobes x {mu.xyz, kappa, weight}. */
+spt_status spt_guide_eval(spt_context* ctx, spt_guide* guide, const float* in, uint32_t n, float* out);
+/* Gradients of the mean weighted negative log-likelihood of n records (host), without updating. */
+spt_status spt_guide_gradients(spt_context* ctx, spt_guide* guide, const spt_guide_record* recs, uint32_t n,
+                               float* grid_grad, float* mlp_grad, float* loss);
+/* One Adam step on n records (host). */
+spt_status spt_guide_train(spt_context* ctx, spt_guide* guide, const spt_guide_record* recs, uint32_t n, float* loss);
+/* Optimiser steps taken by the guide since it was created. */
+spt_status spt_guide_steps(spt_guide* guide, uint64_t* steps);
+/* Guided path tracing: as spt_pathtrace_device, sampling guidable vertices (single-layer Lambertian /
+ * Cook-Torrance) from mix * guide + (1 - mix) * BSDF, and training the guide on its own paths for up to
+ * cfg.max_steps steps. */
+spt_status spt_guided_pathtrace_device(spt_context* ctx, const spt_scene* scene, const spt_camera* cam,
+                                       const spt_pt_params* params, spt_guide* guide, float* d_out_rgb,
+                                       spt_render_stats* stats);
+
 /* ---- image post-processing (reference core/image_buffer.cpp and the ray casters' saveImageToFile) */
 /* sRGB (pow 1/2.2 of the clamped value) + ASCII P3 PPM writer, core/image_buffer.cpp:22-47. */
 spt_status spt_write_ppm(const char* path, const float* rgb, uint32_t width, uint32_t height, int32_t to_srgb);

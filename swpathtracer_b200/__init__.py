@@ -5,5 +5,6 @@ package only loads it (native), mirrors its structs (abi), builds scene descript
 synthetic workloads (scenes) and wraps the handles (api).
 """
 from . import abi, scenes  # noqa: F401
-from .api import Bvh, Device, GpuScene, write_ppm  # noqa: F401
+from .api import (Bvh, Device, GpuScene, Guide, autotune, default_tune, guide_config, render_batch,  # noqa: F401
+                  write_ppm)
 from .native import SptError  # noqa: F401

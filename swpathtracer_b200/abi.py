@@ -94,15 +94,37 @@ class BvhStats(C.Structure):
     ]
 
 
+class Tune(C.Structure):
+    _fields_ = [("capacity", C.c_uint32), ("extend_block", C.c_uint32), ("shade_block", C.c_uint32),
+                ("traversal", C.c_int32), ("check_every", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+
+
+class BatchJob(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("camera", Camera), ("params", PtParams)]
+
+
+class GuideConfig(C.Structure):
+    _fields_ = [("box_min", F3), ("box_max", F3), ("lr", C.c_float), ("batch", C.c_uint32),
+                ("max_steps", C.c_uint32), ("mix", C.c_float), ("seed", C.c_uint64)]
+
+
+GUIDE_LEVELS, GUIDE_FEATS, GUIDE_T = 16, 2, 1 << 19
+GUIDE_GRID_PARAMS = GUIDE_LEVELS * GUIDE_T * GUIDE_FEATS
+GUIDE_MLP_SHAPES = [(64, 48), (64, 64), (64, 64), (64, 64), (48, 64)]
+GUIDE_MLP_PARAMS = sum(a * b for a, b in GUIDE_MLP_SHAPES)
+
+
 # numpy dtypes with the same layout, for bulk arrays crossing the ABI.
 def _np_dtypes():
     import numpy as np
     hit = np.dtype([("t", "<f4"), ("prim_id", "<u4"), ("u", "<f4"), ("v", "<f4")])
     node = np.dtype([("min", "<f4", 3), ("right", "<u4"), ("max", "<f4", 3), ("count", "<u4")])
-    return hit, node
+    rec = np.dtype([("pos", "<f4", 3), ("weight", "<f4"), ("normal", "<f4", 3), ("pad0", "<f4"),
+                    ("wo", "<f4", 3), ("pad1", "<f4"), ("wi", "<f4", 3), ("pad2", "<f4")])
+    return hit, node, rec
 
 
-HIT_DTYPE, BVH2_NODE_DTYPE = _np_dtypes()
+HIT_DTYPE, BVH2_NODE_DTYPE, GUIDE_RECORD_DTYPE = _np_dtypes()
 
 
 def ptr(arr, ctype):

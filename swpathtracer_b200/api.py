@@ -5,6 +5,7 @@ Bvh               spt_bvh, the host-built reference SAH tree (SBVH::build / getS
 GpuScene          spt_scene: a scene resident in HBM, answering ray queries and rendering
 """
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -20,9 +21,16 @@ class Device:
         native.check(self.lib.spt_create(device, C.byref(h)), None, "spt_create(%d)" % device)
         self.h = h
         self.device = device
+        self._children = weakref.WeakSet()   # scenes and guides that live on this context
+
+    def adopt(self, obj):
+        """Registers an object whose handle must be released before the context."""
+        self._children.add(obj)
 
     def close(self):
         if getattr(self, "h", None):
+            for c in list(self._children):
+                c.close()
             self.lib.spt_destroy(self.h)
             self.h = None
 
@@ -80,6 +88,7 @@ class GpuScene:
         device.check(self.lib.spt_scene_create(device.h, packed.ref(), bvh.h if bvh else None, C.byref(h)),
                      "spt_scene_create")
         self.h = h
+        device.adopt(self)
 
     def close(self):
         if getattr(self, "h", None):
@@ -145,6 +154,125 @@ class GpuScene:
         self.dev.check(self.lib.spt_pathtrace_device(self.dev.h, self.h, C.byref(cam), C.byref(params), d_out,
                                                      C.byref(st)), "spt_pathtrace_device")
         return st
+
+    def pathtrace_guided_device(self, cam, params, guide, d_out):
+        """Guided path tracing into the device buffer d_out (float[h][w][3]); the guide trains on the
+        render's own paths for up to its config's max_steps optimiser steps."""
+        st = abi.RenderStats()
+        self.dev.check(self.lib.spt_guided_pathtrace_device(self.dev.h, self.h, C.byref(cam), C.byref(params),
+                                                            guide.h, d_out, C.byref(st)),
+                       "spt_guided_pathtrace_device")
+        return st
+
+
+def default_tune():
+    t = abi.Tune()
+    native.check(native.lib().spt_tune_default(C.byref(t)))
+    return t
+
+
+def _batch_jobs(jobs):
+    arr = (abi.BatchJob * len(jobs))()
+    for i, (scene, cam, params) in enumerate(jobs):
+        arr[i].scene = scene.h.value if hasattr(scene.h, "value") else scene.h
+        arr[i].camera = cam
+        arr[i].params = params
+    return arr
+
+
+def render_batch(device, jobs, d_images, tune=None):
+    """Renders jobs = [(GpuScene, camera, pt_params), ...] in one wavefront into the device buffers
+    d_images (device pointers, float[h][w][3] each).  Returns per-job RenderStats."""
+    arr = _batch_jobs(jobs)
+    ptrs = (C.c_void_p * len(jobs))(*d_images)
+    stats = (abi.RenderStats * len(jobs))()
+    device.check(device.lib.spt_batch_pathtrace(device.h, arr, len(jobs), ptrs, C.byref(tune) if tune else None,
+                                                stats), "spt_batch_pathtrace")
+    return list(stats)
+
+
+def autotune(device, jobs, cache_path=None):
+    """Wavefront settings for this batch, from short timed trials (or the cache file)."""
+    arr = _batch_jobs(jobs)
+    t = abi.Tune()
+    device.check(device.lib.spt_autotune(device.h, arr, len(jobs), cache_path.encode() if cache_path else None,
+                                         C.byref(t)), "spt_autotune")
+    return t
+
+
+def guide_config(box_min=(0, 0, 0), box_max=(1, 1, 1), lr=1e-2, batch=1 << 18, max_steps=64, mix=0.5, seed=1):
+    c = abi.GuideConfig()
+    for k in range(3):
+        c.box_min[k], c.box_max[k] = box_min[k], box_max[k]
+    c.lr, c.batch, c.max_steps, c.mix, c.seed = lr, batch, max_steps, mix, seed
+    return c
+
+
+class Guide:
+    """The neural path-guiding model (hash grid + MLP -> 8 vMF lobes) on one device."""
+
+    def __init__(self, device, config=None):
+        self.dev = device
+        self.lib = device.lib
+        h = C.c_void_p()
+        device.check(self.lib.spt_guide_create(device.h, C.byref(config or guide_config()), C.byref(h)),
+                     "spt_guide_create")
+        self.h = h
+        device.adopt(self)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.spt_guide_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def steps(self):
+        """Optimiser steps taken since creation."""
+        n = C.c_uint64()
+        native.check(self.lib.spt_guide_steps(self.h, C.byref(n)))
+        return n.value
+
+    def get_params(self):
+        grid = np.zeros(abi.GUIDE_GRID_PARAMS, np.float32)
+        mlp = np.zeros(abi.GUIDE_MLP_PARAMS, np.float32)
+        native.check(self.lib.spt_guide_get_params(self.h, grid.ctypes.data, mlp.ctypes.data))
+        return grid, mlp
+
+    def set_params(self, grid=None, mlp=None):
+        g = None if grid is None else np.ascontiguousarray(grid, np.float32)
+        m = None if mlp is None else np.ascontiguousarray(mlp, np.float32)
+        native.check(self.lib.spt_guide_set_params(self.h, None if g is None else g.ctypes.data,
+                                                   None if m is None else m.ctypes.data))
+
+    def eval(self, pos, normal, wo):
+        n = len(pos)
+        x = np.zeros((n, 12), np.float32)
+        x[:, 0:3], x[:, 4:7], x[:, 8:11] = pos, normal, wo
+        out = np.zeros((n, 40), np.float32)
+        self.dev.check(self.lib.spt_guide_eval(self.dev.h, self.h, x.ctypes.data, n, out.ctypes.data), "spt_guide_eval")
+        return out.reshape(n, 8, 5)
+
+    def gradients(self, recs):
+        recs = np.ascontiguousarray(recs, abi.GUIDE_RECORD_DTYPE)
+        grid = np.zeros(abi.GUIDE_GRID_PARAMS, np.float32)
+        mlp = np.zeros(abi.GUIDE_MLP_PARAMS, np.float32)
+        loss = C.c_float()
+        self.dev.check(self.lib.spt_guide_gradients(self.dev.h, self.h, recs.ctypes.data, len(recs), grid.ctypes.data,
+                                                    mlp.ctypes.data, C.byref(loss)), "spt_guide_gradients")
+        return grid, mlp, loss.value
+
+    def train(self, recs):
+        recs = np.ascontiguousarray(recs, abi.GUIDE_RECORD_DTYPE)
+        loss = C.c_float()
+        self.dev.check(self.lib.spt_guide_train(self.dev.h, self.h, recs.ctypes.data, len(recs), C.byref(loss)),
+                       "spt_guide_train")
+        return loss.value
 
 
 def write_ppm(path, rgb, srgb=True):

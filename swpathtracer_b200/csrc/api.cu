@@ -5,7 +5,10 @@
 #include <memory>
 #include <new>
 
+#include <cstdlib>
+
 #include "spt_internal.h"
+#include "wide_build.h"
 
 namespace spt {
 
@@ -42,6 +45,21 @@ spt_status pinned(spt_context* ctx, size_t bytes, void** out) {
     }
     *out = ctx->pinned;
     return SPT_OK;
+}
+
+spt_status fetch_counter(spt_context* ctx, cudaStream_t s, unsigned long long** out) {
+    if (!ctx->d_fetch) SPT_CUDA(ctx, cudaMalloc(&ctx->d_fetch, kFetchRing * sizeof(unsigned long long)));
+    unsigned long long* c = ctx->d_fetch + (ctx->fetch_slot++ % kFetchRing);
+    SPT_CUDA(ctx, cudaMemsetAsync(c, 0, sizeof(unsigned long long), s));
+    *out = c;
+    return SPT_OK;
+}
+
+int persistent_grid(spt_context* ctx, const void* kernel, int block) {
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1) per_sm = 1;
+    return sms * per_sm;
 }
 
 spt_status check_status(spt_context* ctx) {
@@ -197,6 +215,7 @@ spt_status spt_destroy(spt_context* ctx) {
         if (ctx->scratch[i]) cudaFree(ctx->scratch[i]);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->d_fetch) cudaFree(ctx->d_fetch);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -367,6 +386,33 @@ spt_status spt_scene_create(spt_context* ctx, const spt_scene_desc* d, const spt
                 r[2] = make_float4(p[6] - p[0], p[7] - p[1], p[8] - p[2], bits_f(d->prim_type[i]));
             }
         }
+        // 8-wide quantized tree over the same leaves (traverse_wide.cuh)
+        std::vector<WideNode> wnodes;
+        std::vector<float4> wtri;
+        if (tree) {
+            WideBvh wb;
+            build_wide(tree->nodes, wb);
+            wnodes.swap(wb.nodes);
+            wtri.resize(3ull * wb.tri_rank.size());
+            for (size_t k = 0; k < wb.tri_rank.size(); ++k) {
+                const uint32_t rk = wb.tri_rank[k];
+                const float4* r = &tri[3ull * rk];
+                const uint32_t type = d->prim_type[slot_prim[rk]];
+                if (type == SPT_PRIM_SPHERE) {
+                    wtri[3 * k] = make_float4(r[0].x, r[0].y, r[0].z, bits_f(rk));
+                    wtri[3 * k + 1] = make_float4(0.0f, 0.0f, 0.0f, bits_f(type));
+                    wtri[3 * k + 2] = make_float4(r[1].x, 0.0f, 0.0f, r[1].w);
+                } else {
+                    wtri[3 * k] = make_float4(r[0].x, r[0].y, r[0].z, bits_f(rk));
+                    wtri[3 * k + 1] = make_float4(r[1].x, r[1].y, r[1].z, bits_f(type));
+                    wtri[3 * k + 2] = make_float4(r[2].x, r[2].y, r[2].z, r[1].w);  // leaf id
+                }
+            }
+            const char* env = std::getenv("SPT_TRAVERSAL");
+            S.traversal = 2;  // wide nodes, persistent dynamic fetch where a kernel supports it
+            if (env && std::string(env) == "binary") S.traversal = 0;
+            if (env && std::string(env) == "wide") S.traversal = 1;
+        }
         // materials
         std::vector<DevBsdf> bs(d->n_bsdfs);
         for (uint32_t i = 0; i < d->n_bsdfs; ++i) {
@@ -410,6 +456,15 @@ spt_status spt_scene_create(spt_context* ctx, const spt_scene_desc* d, const spt
         if ((s = upload(sc.get(), bs, &S.bsdf)) != SPT_OK) return s;
         if ((s = upload(sc.get(), ms, &S.mat)) != SPT_OK) return s;
         if ((s = upload(sc.get(), layers, &S.layer_ids)) != SPT_OK) return s;
+        {
+            const uint4* wn = nullptr;
+            std::vector<uint4> raw(wnodes.size() * 5);
+            if (!wnodes.empty()) std::memcpy(raw.data(), wnodes.data(), wnodes.size() * sizeof(WideNode));
+            if ((s = upload(sc.get(), raw, &wn)) != SPT_OK) return s;
+            S.wnode = wn;
+            S.n_wnodes = static_cast<uint32_t>(wnodes.size());
+            if ((s = upload(sc.get(), wtri, &S.wtri)) != SPT_OK) return s;
+        }
         *out = sc.release();
         return SPT_OK;
     } catch (const std::bad_alloc&) {

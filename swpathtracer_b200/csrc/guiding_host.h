@@ -1,0 +1,52 @@
+// guiding_host.h -- host-side state of the path-guiding model (guiding.cu).
+#pragma once
+
+#include <vector>
+
+#include "guiding.cuh"
+#include "spt_internal.h"
+
+namespace spt {
+namespace guide {
+
+size_t infer_smem_bytes();
+size_t train_smem_bytes();
+
+struct Guide {
+    spt_context* ctx = nullptr;
+    spt_guide_config cfg{};
+    Model model{};
+    float *grid_master = nullptr, *grid_m = nullptr, *grid_v = nullptr, *grid_grad = nullptr;
+    __nv_bfloat16* grid_bf16 = nullptr;
+    float *mlp_master = nullptr, *mlp_m = nullptr, *mlp_v = nullptr, *mlp_grad = nullptr;
+    __nv_bfloat16* smem_image = nullptr;
+    float* scalars = nullptr;  // [0] mean weight, [1] loss sum
+    uint32_t steps = 0;
+    std::vector<void*> allocations;
+    // training scratch
+    __nv_bfloat16* xt[kLayers] = {};
+    __nv_bfloat16* dzt[kLayers] = {};
+    float* partial = nullptr;
+    uint32_t train_cap = 0;
+    std::vector<void*> train_allocs;
+
+    spt_status alloc(spt_context* c, const spt_guide_config& cfg);
+    spt_status refresh();
+    spt_status infer(const float4* d_in, uint32_t n, float* d_out, cudaStream_t s);
+    // inference for a device-side count of samples (at most max_n); usable inside a CUDA graph
+    spt_status infer_list(const float4* d_in, const uint32_t* d_n, uint32_t max_n, float* d_out, cudaStream_t s);
+    spt_status ensure_train_buffers(uint32_t n);
+    spt_status gradients(const float4* d_rec, uint32_t n);
+    spt_status step(const float4* d_rec, uint32_t n, float* loss);
+    ~Guide() {
+        for (void* p : train_allocs) cudaFree(p);
+        for (void* p : allocations) cudaFree(p);
+    }
+};
+
+}  // namespace guide
+}  // namespace spt
+
+struct spt_guide {
+    spt::guide::Guide g;
+};

@@ -1,180 +1,370 @@
-// pathtrace.cu -- the path tracer (integrators/pathtracer.cpp:12-147) as a wavefront.
+// pathtrace.cu -- the path tracer (integrators/pathtracer.cpp:12-147) as a wavefront over a batch
+// of scenes.
 //
-// A fixed pool of path slots (SoA, ping-pong) is refilled with new camera paths as old ones end:
+// A pool of path slots (SoA, ping-pong) is refilled with new camera paths as old ones end.  Each
+// iteration runs four kernels:
 //
 //   k_generate  camera rays for free slots (pixel sampler + camera, pathtracer.cpp:104-113)
-//   k_extend    closest hit for every live slot (traverse.cuh; the same kernel code as the ray casters)
+//   k_extend    closest hit for every live slot (traverse*.cuh, the ray casters' traversal)
 //   k_shade     emission, layered BSDF walk, russian roulette and the next ray
 //               (pathtracer.cpp:21-54); surviving paths are appended, warp-aggregated, to the other
-//               buffer; finished paths add their radiance to the image
+//               buffer; finished paths add their radiance to their scene's image
 //   k_advance   one thread: moves the counters to the next iteration
 //
-// Random numbers: Philox-4x32-10 keyed by the seed, counter (path index, stream, block), stream 0
+// A batch is a table of jobs (scene + camera + settings); the camera paths of all jobs form one index
+// space, so scenes of very different sizes share the pool, and the iterations are replayed from one
+// CUDA graph.  A single-scene render is a batch of one.
+//
+// Random numbers: Philox-4x32-10 keyed by the job's seed, counter (path index, stream, block), stream 0
 // for the pixel sample and stream depth+1 for the BSDF walk and roulette at that depth.  The path
-// index is (spp_offset + sample) * viewport_pixels + viewport_pixel, so an image does not depend
-// on slot assignment or scheduling (up to the order of the float atomic adds into the image).
+// index is (spp_offset + sample) * viewport_pixels + viewport_pixel, so an image does not depend on
+// slot assignment, batch composition or tuning (up to the order of the float atomic adds).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <vector>
 
+#include "guided_shade.cuh"
+#include "guiding_host.h"
 #include "shade.cuh"
 #include "spt_internal.h"
-#include "traverse.cuh"
+#include "traverse_wide.cuh"
+#include "wavefront.h"
 
 namespace spt {
 namespace {
 
-struct PtConst {
-    DevScene S;
-    DevCamera cam;
-    uint64_t seed;
-    uint64_t total;        // camera paths to trace
-    uint32_t spp, nsub;    // samples per pixel (after the square rounding), strata per axis
-    float sw;              // stratum width
-    int sampler, rr, path_length, cap;
-    uint32_t npix;         // viewport pixels
-    uint32_t spp_offset;
+struct Wave {
+    const PtJob* jobs;
+    uint32_t n_jobs;
+    uint64_t total;        // camera paths of all jobs
     uint32_t capacity;     // path slots
-    float* image;          // W*H*3 radiance sums
 };
 
 struct PathBuf {
     float4* o;   // origin, pixel (viewport index) bits
     float4* d;   // direction, sample index bits
-    float4* b;   // throughput, depth bits
+    float4* b;   // throughput, depth | job << 16
     float4* l;   // radiance so far
+    uint4* r;    // guided renders: the path's last four training records (generation << 24 | index)
 };
 
 struct Counters {
     unsigned long long next_path;   // camera paths generated so far
     unsigned long long segments;    // rays traced so far
+    unsigned long long fetch;       // ray counter of the persistent extend kernel
     uint32_t n_alive;               // live slots at the start of the iteration (in the current buffer)
     uint32_t n_next;                // slots appended to the other buffer by k_shade
     uint32_t iterations;
+    uint32_t n_guided;              // guided renders: hits listed for the guide this iteration
+    uint32_t rec_count;             // training records written into the current generation
+    uint32_t rec_gen;               // generation of the record buffer (bumped when it is consumed)
+    uint32_t train_on;              // record training data
     uint32_t pad;
 };
 
-__device__ __forceinline__ uint32_t n_new_paths(const PtConst& C, const Counters& c) {
-    const unsigned long long rem = C.total - c.next_path;
-    const uint32_t room = C.capacity - c.n_alive;
+// Guided renders (guided_shade.cuh): the guide's inputs and outputs for this iteration's hits and the
+// training-record buffers.
+struct GuideIO {
+    float mix;
+    uint32_t rec_cap;
+    float4* infer_in;      // 3 float4 per listed hit: position, normal, outgoing direction
+    float* lobes;          // 40 floats per listed hit
+    uint32_t* slot_list;   // slot -> list index, or ~0
+    float4* rec;           // 4 float4 per record (spt_guide_record layout)
+    float4* recx;          // 2 float4 per record: throughput at the record, radiance gathered after it
+};
+
+constexpr uint32_t kNoRec = 0xFFFFFFFFu;
+constexpr uint32_t kRecBatches = 4;   // training records held per render: this many optimiser batches
+
+__device__ __forceinline__ uint32_t n_new_paths(const Wave& W, const Counters& c) {
+    const unsigned long long rem = W.total - c.next_path;
+    const uint32_t room = W.capacity - c.n_alive;
     return rem < room ? static_cast<uint32_t>(rem) : room;
 }
 
-__global__ void __launch_bounds__(256) k_generate(PtConst C, const Counters* __restrict__ ctr, PathBuf cur) {
+__device__ __forceinline__ uint32_t job_of(const Wave& W, unsigned long long g) {
+    uint32_t lo = 0, hi = W.n_jobs;  // last job with first <= g
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (W.jobs[mid].first <= g) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) k_generate(Wave W, const Counters* __restrict__ ctr, PathBuf cur) {
     const Counters c = *ctr;
-    const uint32_t n_new = n_new_paths(C, c);
+    const uint32_t n_new = n_new_paths(W, c);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x) {
         const unsigned long long g = c.next_path + i;
-        const uint32_t si = static_cast<uint32_t>(g / C.npix);
-        const uint32_t pix = static_cast<uint32_t>(g - static_cast<unsigned long long>(si) * C.npix);
-        const uint32_t xx = pix % C.cam.vp_width, yy = pix / C.cam.vp_width;
-        const uint32_t x = C.cam.vp_left + xx, y = C.cam.vp_top + yy;
-        const uint32_t sg = C.spp_offset + si;
-        const unsigned long long path = static_cast<unsigned long long>(sg) * C.npix + pix;
+        const uint32_t j = job_of(W, g);
+        const PtJob& J = W.jobs[j];
+        const unsigned long long lg = g - J.first;
+        const uint32_t sr = static_cast<uint32_t>(lg / J.npix);
+        const uint32_t pix = static_cast<uint32_t>(lg - static_cast<unsigned long long>(sr) * J.npix);
+        const uint32_t si = J.s_begin + sr;   // sample index within the pixel's spp
+        const uint32_t xx = pix % J.cam.vp_width, yy = pix / J.cam.vp_width;
+        const uint32_t x = J.cam.vp_left + xx, y = J.cam.vp_top + yy;
+        const uint32_t sg = J.spp_offset + si;
+        const unsigned long long path = static_cast<unsigned long long>(sg) * J.npix + pix;
         float sx, sy;
-        if (C.sampler == SPT_PIXEL_UNIFORM) {  // uniform_pixel_sampler.cpp:7-10
-            Stream cs(C.seed, path, 0);
+        if (J.sampler == SPT_PIXEL_UNIFORM) {  // uniform_pixel_sampler.cpp:7-10
+            Stream cs(J.seed, path, 0);
             sx = cs.next();
             sy = cs.next();
         } else {
-            const uint32_t a = si / C.nsub, b = si % C.nsub;
-            if (C.sampler == SPT_PIXEL_REGULAR) {  // regular_pixel_sampler.cpp:10-13
-                float off = C.sw * 0.5f;
-                sx = C.sw * a + off;
-                sy = C.sw * b + off;
+            const uint32_t a = si / J.nsub, b = si % J.nsub;
+            if (J.sampler == SPT_PIXEL_REGULAR) {  // regular_pixel_sampler.cpp:10-13
+                float off = J.sw * 0.5f;
+                sx = J.sw * a + off;
+                sy = J.sw * b + off;
             } else {  // jittered_pixel_sampler.cpp:11-20
-                Stream cs(C.seed, path, 0);
+                Stream cs(J.seed, path, 0);
                 float u0 = cs.next(), u1 = cs.next();
-                sx = C.sw * a + C.sw * u0;
-                sy = C.sw * b + C.sw * u1;
+                sx = J.sw * a + J.sw * u0;
+                sy = J.sw * b + J.sw * u1;
             }
         }
         V3 o, d;
-        camera_ray(C.cam, static_cast<float>(x) + sx, static_cast<float>(y) + sy, o, d);
+        camera_ray(J.cam, static_cast<float>(x) + sx, static_cast<float>(y) + sy, o, d);
         const uint32_t slot = c.n_alive + i;
         cur.o[slot] = make_float4(o.x, o.y, o.z, __uint_as_float(pix));
         cur.d[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(sg));
-        cur.b[slot] = make_float4(1.0f, 1.0f, 1.0f, __int_as_float(0));
+        cur.b[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(j << 16));
         cur.l[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (cur.r) cur.r[slot] = make_uint4(kNoRec, kNoRec, kNoRec, kNoRec);
     }
 }
 
-__global__ void __launch_bounds__(128) k_extend(PtConst C, const Counters* __restrict__ ctr, PathBuf cur,
+// Guided renders: list this iteration's hits on guidable materials and the guide's inputs for them.
+__global__ void __launch_bounds__(256) k_guide_collect(Wave W, Counters* __restrict__ ctr, PathBuf cur,
+                                                      const float4* __restrict__ hits, GuideIO G) {
+    const Counters c = *ctr;
+    const uint32_t n = c.n_alive + n_new_paths(W, c);
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        bool take = false;
+        float4 p4, n4, w4;
+        if (i < n) {
+            const float4 h4 = hits[i];
+            const uint32_t prim = __float_as_uint(h4.y);
+            if (prim != SPT_MISS) {
+                const PtJob& J = W.jobs[__float_as_uint(cur.b[i].w) >> 16];
+                const DevMaterial m = J.S.mat[J.S.prim_mat[prim]];
+                if (guidable(J.S, m)) {
+                    const V3 o = f3v(cur.o[i]), d = f3v(cur.d[i]);
+                    const V3 pos = hit_pos(J.S.prim_type[prim] == SPT_PRIM_SPHERE, o, d, h4.x);
+                    const V3 nrm = hit_normal(J.S, prim, h4.z, h4.w, pos);
+                    p4 = make_float4(pos.x, pos.y, pos.z, 0.0f);
+                    n4 = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
+                    w4 = make_float4(-d.x, -d.y, -d.z, 0.0f);
+                    take = true;
+                }
+            }
+            if (!take) G.slot_list[i] = kNoRec;
+        }
+        const unsigned mask = __ballot_sync(0xFFFFFFFFu, take);
+        if (mask) {
+            uint32_t first = 0;
+            if (lane == 0) first = atomicAdd(&ctr->n_guided, static_cast<uint32_t>(__popc(mask)));
+            first = __shfl_sync(0xFFFFFFFFu, first, 0);
+            if (take) {
+                const uint32_t k = first + __popc(mask & ((1u << lane) - 1u));
+                G.slot_list[i] = k;
+                G.infer_in[3 * k] = p4;
+                G.infer_in[3 * k + 1] = n4;
+                G.infer_in[3 * k + 2] = w4;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ float4 hit_record(const DevScene& S, const Hit1& h) {
+    return make_float4(h.t, __uint_as_float(h.found ? slot_prim(S, h.slot) : SPT_MISS), h.u, h.v);
+}
+
+template <int TRAV>
+__global__ void __launch_bounds__(256) k_extend(Wave W, const Counters* __restrict__ ctr, PathBuf cur,
                                                 float4* __restrict__ hits, uint32_t* status) {
     const Counters c = *ctr;
-    const uint32_t n = c.n_alive + n_new_paths(C, c);
+    const uint32_t n = c.n_alive + n_new_paths(W, c);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 o = cur.o[i], d = cur.d[i];
-        Hit1 h = closest_hit<kStack>(C.S, f3v(o), f3v(d), status);
-        hits[i] = make_float4(h.t, __uint_as_float(h.found ? slot_prim(C.S, h.slot) : SPT_MISS), h.u, h.v);
+        const DevScene& S = W.jobs[__float_as_uint(cur.b[i].w) >> 16].S;
+        Hit1 h = trace_closest<TRAV>(S, f3v(o), f3v(d), status);
+        hits[i] = hit_record(S, h);
     }
 }
 
-__device__ __forceinline__ void splat(const PtConst& C, uint32_t pix, V3 L) {
-    const uint32_t x = C.cam.vp_left + pix % C.cam.vp_width, y = C.cam.vp_top + pix / C.cam.vp_width;
-    float* p = C.image + 3ull * (static_cast<uint64_t>(y) * C.cam.width + x);
+// Persistent extend: lanes take live slots from the iteration's counter as their rays finish.
+__global__ void __launch_bounds__(128) k_extend_df(Wave W, Counters* __restrict__ ctr, PathBuf cur,
+                                                   float4* __restrict__ hits, uint32_t* status) {
+    const Counters c = *ctr;
+    const uint32_t n = c.n_alive + n_new_paths(W, c);
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    WideTraversal tr;
+    const DevScene* S = nullptr;
+    bool active = false, exhausted = false;
+    unsigned long long mine = 0, pool = 0, pool_end = 0;
+    for (;;) {
+        const unsigned need = __ballot_sync(0xFFFFFFFFu, !active && !exhausted);
+        if (need) {
+            const uint32_t cnt = __popc(need), rank = __popc(need & lt);
+            const unsigned long long have = pool_end - pool;
+            unsigned long long fresh = 0;
+            if (have < cnt) {
+                if (lane == 0) fresh = atomicAdd(&ctr->fetch, static_cast<unsigned long long>(kChunk));
+                fresh = __shfl_sync(0xFFFFFFFFu, fresh, 0);
+            }
+            if (!active && !exhausted) {
+                mine = rank < have ? pool + rank : fresh + (rank - have);
+                if (mine >= n) {
+                    exhausted = true;
+                } else {
+                    S = &W.jobs[__float_as_uint(cur.b[mine].w) >> 16].S;
+                    active = tr.start(*S, f3v(cur.o[mine]), f3v(cur.d[mine]));
+                    if (!active) hits[mine] = hit_record(*S, tr.h);
+                }
+            }
+            if (have < cnt) {
+                pool = fresh + (cnt - have);
+                pool_end = fresh + kChunk;
+            } else {
+                pool += cnt;
+            }
+        }
+        if (__all_sync(0xFFFFFFFFu, !active && exhausted)) break;
+        if (active && !tr.step(*S, status)) {
+            if (tr.finish(*S)) {
+                hits[mine] = hit_record(*S, tr.h);
+                active = false;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void splat(const PtJob& J, uint32_t pix, V3 L) {
+    const uint32_t x = J.cam.vp_left + pix % J.cam.vp_width, y = J.cam.vp_top + pix / J.cam.vp_width;
+    float* p = J.image + 3ull * (static_cast<uint64_t>(y) * J.cam.width + x);
     if (L.x != 0.0f) atomicAdd(p, L.x);
     if (L.y != 0.0f) atomicAdd(p + 1, L.y);
     if (L.z != 0.0f) atomicAdd(p + 2, L.z);
 }
 
-__global__ void __launch_bounds__(128) k_shade(PtConst C, Counters* __restrict__ ctr, PathBuf cur, PathBuf nxt,
-                                               const float4* __restrict__ hits) {
+__device__ __forceinline__ bool rec_live(uint32_t r, uint32_t gen) { return r != kNoRec && (r >> 24) == (gen & 0xFFu); }
+
+template <bool GUIDED>
+__global__ void __launch_bounds__(256) k_shade(Wave W, Counters* __restrict__ ctr, PathBuf cur, PathBuf nxt,
+                                               const float4* __restrict__ hits, GuideIO G) {
     const Counters c = *ctr;
-    const uint32_t n = c.n_alive + n_new_paths(C, c);
+    const uint32_t n = c.n_alive + n_new_paths(W, c);
     const uint32_t lane = threadIdx.x & 31;
     // all lanes of a warp iterate together so the append below can be warp-aggregated
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const uint32_t i = base + threadIdx.x;
         bool keep = false;
         float4 wo_o, wo_d, wo_b, wo_l;
+        uint4 rr = make_uint4(kNoRec, kNoRec, kNoRec, kNoRec);
         if (i < n) {
             const float4 o4 = cur.o[i], d4 = cur.d[i], b4 = cur.b[i], l4 = cur.l[i], h4 = hits[i];
+            if (GUIDED) rr = cur.r[i];
             const uint32_t pix = __float_as_uint(o4.w), sg = __float_as_uint(d4.w);
-            const int depth = __float_as_int(b4.w);
-            const uint64_t path = static_cast<uint64_t>(sg) * C.npix + pix;
+            const uint32_t jd = __float_as_uint(b4.w);
+            const int depth = static_cast<int>(jd & 0xFFFFu);
+            const PtJob& J = W.jobs[jd >> 16];
+            const uint64_t path = static_cast<uint64_t>(sg) * J.npix + pix;
             const V3 o = f3v(o4), d = f3v(d4);
             V3 beta = f3v(b4), L = f3v(l4);
             const uint32_t prim = __float_as_uint(h4.y);
             bool done = false;
             if (prim == SPT_MISS) {  // pathtracer.cpp:21-26
-                if (depth == 0) L = L + beta * v3(C.S.bg[0], C.S.bg[1], C.S.bg[2]);
+                if (depth == 0) L = L + beta * v3(J.S.bg[0], J.S.bg[1], J.S.bg[2]);
                 done = true;
             } else {
                 const float t = h4.x;
-                const bool sphere = C.S.prim_type[prim] == SPT_PRIM_SPHERE;
+                const bool sphere = J.S.prim_type[prim] == SPT_PRIM_SPHERE;
                 const V3 pos = hit_pos(sphere, o, d, t);
-                const V3 nrm = hit_normal(C.S, prim, h4.z, h4.w, pos);
-                const DevMaterial m = C.S.mat[C.S.prim_mat[prim]];
+                const V3 nrm = hit_normal(J.S, prim, h4.z, h4.w, pos);
+                const DevMaterial m = J.S.mat[J.S.prim_mat[prim]];
                 float frame[9];
                 onb_from_normal(nrm, frame);                       // pathtracer.cpp:28-30
                 const V3 wo = normalize(mat_tmul(frame, -d));
-                Stream bs(C.seed, path, static_cast<uint32_t>(depth) + 1u);
-                LayerEval e = eval_layered(C.S, m, wo, bs);
-                const V3 wwi = mat_mul(frame, e.wi);               // pathtracer.cpp:37-38
+                Stream bs(J.seed, path, static_cast<uint32_t>(depth) + 1u);
+                V3 f, refl, wi, wwi;
+                float pdf;
+                const uint32_t gi = GUIDED ? G.slot_list[i] : kNoRec;
+                if (GUIDED && gi != kNoRec) {
+                    const GuidedSample gs = guided_sample(J.S, m, frame, wo, G.lobes + 40ull * gi, G.mix, bs);
+                    f = gs.f;
+                    refl = gs.refl;
+                    wi = gs.wi_local;
+                    wwi = gs.wi_world;
+                    pdf = gs.p;
+                    if (!(pdf > 0.0f)) {
+                        f = v3(0.0f, 0.0f, 0.0f);
+                        pdf = 1.0f;
+                    }
+                } else {
+                    const LayerEval e = eval_layered(J.S, m, wo, bs);
+                    f = e.f;
+                    refl = e.refl;
+                    wi = e.wi;
+                    pdf = e.pdf;
+                    wwi = mat_mul(frame, e.wi);                    // pathtracer.cpp:37-38
+                }
                 const V3 no = pos + wwi * 1e-3f;
-                L = L + beta * v3(m.er, m.eg, m.eb);
-                const float k = fmaxf(fmaxf(e.refl.x, e.refl.y), e.refl.z);
-                if (C.rr && depth >= C.path_length) {              // pathtracer.cpp:43-49
-                    if ((bs.next() < k) && (depth < C.cap)) e.f = e.f / k;
+                const V3 le = v3(m.er, m.eg, m.eb);
+                if (GUIDED && (le.x != 0.0f || le.y != 0.0f || le.z != 0.0f)) {
+                    // radiance reaching the path's open training records
+                    const V3 add = beta * le;
+                    const uint32_t ids[4] = {rr.x, rr.y, rr.z, rr.w};
+                    for (int k = 0; k < 4; ++k)
+                        if (rec_live(ids[k], c.rec_gen)) {
+                            float4* sx = G.recx + 2ull * (ids[k] & 0xFFFFFFu) + 1;
+                            const float4 v = *sx;
+                            *sx = make_float4(v.x + add.x, v.y + add.y, v.z + add.z, 0.0f);
+                        }
+                }
+                L = L + beta * le;
+                const float k = fmaxf(fmaxf(refl.x, refl.y), refl.z);
+                if (J.rr && depth >= J.path_length) {              // pathtracer.cpp:43-49
+                    if ((bs.next() < k) && (depth < J.cap)) f = f / k;
                     else done = true;
-                } else if (C.rr && depth >= C.cap) {
+                } else if (J.rr && depth >= J.cap) {
                     done = true;
                 }
                 if (!done) {
-                    beta = ((beta * e.f) * e.wi.y) / e.pdf;        // pathtracer.cpp:52-54
+                    const V3 beta0 = beta;
+                    beta = ((beta * f) * wi.y) / pdf;              // pathtracer.cpp:52-54
                     if ((beta.x == 0.0f && beta.y == 0.0f && beta.z == 0.0f) ||
-                        (!C.rr && depth + 1 >= C.path_length)) {   // the next trace would return 0
+                        (!J.rr && depth + 1 >= J.path_length)) {   // the next trace would return 0
                         done = true;
                     } else {
+                        if (GUIDED && gi != kNoRec && c.train_on) {
+                            const uint32_t r = atomicAdd(&ctr->rec_count, 1u);
+                            if (r < G.rec_cap) {
+                                G.rec[4ull * r] = make_float4(pos.x, pos.y, pos.z, 0.0f);
+                                G.rec[4ull * r + 1] = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
+                                G.rec[4ull * r + 2] = make_float4(-d.x, -d.y, -d.z, 0.0f);
+                                G.rec[4ull * r + 3] = make_float4(wwi.x, wwi.y, wwi.z, 0.0f);
+                                G.recx[2ull * r] = make_float4(beta0.x, beta0.y, beta0.z, 0.0f);
+                                G.recx[2ull * r + 1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                                rr = make_uint4(((c.rec_gen & 0xFFu) << 24) | r, rr.x, rr.y, rr.z);
+                            }
+                        }
                         keep = true;
                         wo_o = make_float4(no.x, no.y, no.z, o4.w);
                         wo_d = make_float4(wwi.x, wwi.y, wwi.z, d4.w);
-                        wo_b = make_float4(beta.x, beta.y, beta.z, __int_as_float(depth + 1));
+                        wo_b = make_float4(beta.x, beta.y, beta.z, __uint_as_float(jd + 1u));
                         wo_l = make_float4(L.x, L.y, L.z, 0.0f);
                     }
                 }
             }
-            if (done) splat(C, pix, L);
+            if (done) splat(J, pix, L);
         }
         const unsigned mask = __ballot_sync(0xFFFFFFFFu, keep);
         if (mask) {
@@ -187,20 +377,41 @@ __global__ void __launch_bounds__(128) k_shade(PtConst C, Counters* __restrict__
                 nxt.d[slot] = wo_d;
                 nxt.b[slot] = wo_b;
                 nxt.l[slot] = wo_l;
+                if (GUIDED) nxt.r[slot] = rr;
             }
         }
     }
 }
 
-__global__ void k_advance(PtConst C, Counters* ctr) {
+__global__ void k_advance(Wave W, Counters* ctr) {
     Counters c = *ctr;
-    const uint32_t n_new = n_new_paths(C, c);
+    const uint32_t n_new = n_new_paths(W, c);
     c.segments += c.n_alive + n_new;
     c.next_path += n_new;
     c.n_alive = c.n_next;
     c.n_next = 0;
+    c.fetch = 0;
+    c.n_guided = 0;
     c.iterations += 1;
     *ctr = c;
+}
+
+// Training weight of every record: luminance of (radiance gathered after the record / throughput at it),
+// i.e. the path's estimate of f cos Li / p at the record.
+__global__ void k_record_weights(float4* __restrict__ rec, const float4* __restrict__ recx, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 b = recx[2 * i], sx = recx[2 * i + 1];
+        const float r = b.x > 0.0f ? sx.x / b.x : 0.0f, g = b.y > 0.0f ? sx.y / b.y : 0.0f,
+                    bl = b.z > 0.0f ? sx.z / b.z : 0.0f;
+        const float w = 0.2126f * r + 0.7152f * g + 0.0722f * bl;
+        rec[4 * i].w = fminf(fmaxf(w, 0.0f), 1e3f);
+    }
+}
+
+__global__ void k_next_generation(Counters* ctr, uint32_t train_on) {
+    ctr->rec_count = 0;
+    ctr->rec_gen += 1;
+    ctr->train_on = train_on;
 }
 
 __global__ void k_finalize(float* image, uint64_t n, float inv_spp) {
@@ -211,6 +422,243 @@ __global__ void k_finalize(float* image, uint64_t n, float inv_spp) {
 
 }  // namespace
 
+spt_status make_job(spt_context* ctx, const spt_scene* sc, const spt_camera* cam, const spt_pt_params* p, float* d_image,
+                    PtJob& J) {
+    if (!sc || !cam || !p || !d_image) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (p->pixel_sampler < SPT_PIXEL_UNIFORM || p->pixel_sampler > SPT_PIXEL_JITTERED)
+        return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "unknown pixel sampler");
+    if (p->termination != SPT_TERMINATE_MAX_DEPTH && p->termination != SPT_TERMINATE_RUSSIAN_ROULETTE)
+        return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "unknown path termination criterion");
+    if (p->spp == 0) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "spp must be > 0");
+    if (p->path_length < 0 || p->max_depth < 0) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "negative path length");
+    std::memset(&J, 0, sizeof(J));
+    spt_status st = make_camera(ctx, cam, J.cam);
+    if (st != SPT_OK) return st;
+    J.S = sc->dev;
+    J.seed = p->seed;
+    J.sampler = p->pixel_sampler;
+    J.spp = p->spp;
+    J.nsub = 1;
+    J.sw = 1.0f;
+    if (p->pixel_sampler != SPT_PIXEL_UNIFORM) {  // regular/jittered round spp up to a square
+        J.nsub = static_cast<uint32_t>(std::ceil(std::sqrt(static_cast<double>(p->spp))));
+        J.spp = J.nsub * J.nsub;
+        J.sw = 1.0f / J.nsub;
+    }
+    J.rr = p->termination == SPT_TERMINATE_RUSSIAN_ROULETTE;
+    J.path_length = p->path_length;
+    J.cap = p->max_depth > 0 ? p->max_depth - 1 : 1000;
+    if (J.cap > 0xFFFE) J.cap = 0xFFFE;  // depth is kept in 16 bits
+    J.npix = J.cam.vp_width * J.cam.vp_height;
+    J.spp_offset = p->spp_offset;
+    J.image = d_image;
+    set_sample_range(J, 0, J.spp);
+    return SPT_OK;
+}
+
+void set_sample_range(PtJob& J, uint32_t s_begin, uint32_t s_end) {
+    J.s_end = std::min(s_end, J.spp);
+    J.s_begin = std::min(s_begin, J.s_end);
+    const bool empty = !J.rr && J.path_length <= 0;   // the reference traces nothing at all then
+    J.total = empty ? 0 : static_cast<uint64_t>(J.npix) * (J.s_end - J.s_begin);
+}
+
+spt_tune default_tune() {
+    spt_tune t;
+    std::memset(&t, 0, sizeof(t));
+    t.capacity = 1u << 21;
+    t.extend_block = 128;
+    t.shade_block = 128;
+    t.traversal = -1;
+    t.check_every = 8;
+    return t;
+}
+
+spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tune& tune, uint64_t* segments,
+                       float* gpu_ms, guide::Guide* guide, uint32_t train_budget, uint32_t* train_steps) {
+    SPT_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (jobs.empty() || jobs.size() >= (1u << 16))
+        return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "a batch holds 1 to 65535 jobs");
+    auto block_ok = [](uint32_t b) { return b == 0 || (b % 32 == 0 && b <= 256); };
+    if (!block_ok(tune.extend_block) || !block_ok(tune.shade_block))
+        return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "tune block sizes must be multiples of 32 up to 256");
+    if (tune.traversal < -1 || tune.traversal > 2) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "unknown traversal");
+    if (train_steps) *train_steps = 0;
+    uint64_t total = 0;
+    int trav = 2;
+    for (PtJob& J : jobs) {
+        J.first = total;
+        total += J.total;
+        if (J.total) trav = std::min(trav, J.S.traversal);  // a scene without a wide tree forces binary
+        const uint64_t img_elems = 3ull * J.cam.width * J.cam.height;
+        if (J.s_begin == 0) SPT_CUDA(ctx, cudaMemsetAsync(J.image, 0, img_elems * sizeof(float), ctx->stream));
+    }
+    if (tune.traversal >= 0 && tune.traversal <= trav) trav = tune.traversal;
+    *segments = 0;
+    *gpu_ms = 0.0f;
+    if (total == 0) return check_status(ctx);
+    const uint64_t cap = std::min<uint64_t>(total, std::max<uint32_t>(tune.capacity, 1024u));
+    spt_status st;
+    void* mem;
+    const size_t buf_bytes = cap * sizeof(float4);
+    const size_t job_bytes = jobs.size() * sizeof(PtJob);
+    if ((st = scratch(ctx, 5, buf_bytes * 9 + sizeof(Counters) + job_bytes + 512, &mem)) != SPT_OK) return st;
+    char* base = static_cast<char*>(mem);
+    PathBuf A{reinterpret_cast<float4*>(base), reinterpret_cast<float4*>(base + buf_bytes),
+              reinterpret_cast<float4*>(base + 2 * buf_bytes), reinterpret_cast<float4*>(base + 3 * buf_bytes), nullptr};
+    PathBuf B{reinterpret_cast<float4*>(base + 4 * buf_bytes), reinterpret_cast<float4*>(base + 5 * buf_bytes),
+              reinterpret_cast<float4*>(base + 6 * buf_bytes), reinterpret_cast<float4*>(base + 7 * buf_bytes),
+              nullptr};
+    float4* hits = reinterpret_cast<float4*>(base + 8 * buf_bytes);
+    Counters* d_ctr = reinterpret_cast<Counters*>(base + 9 * buf_bytes);
+    PtJob* d_jobs = reinterpret_cast<PtJob*>(base + 9 * buf_bytes + 256);
+    SPT_CUDA(ctx, cudaMemsetAsync(d_ctr, 0, sizeof(Counters), ctx->stream));
+    SPT_CUDA(ctx, cudaMemcpyAsync(d_jobs, jobs.data(), job_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    GuideIO G{};
+    uint32_t batch = 0, rec_cap = 0;
+    if (guide) {
+        // guided state: record ids per path, the guide's per-hit inputs/outputs, training records
+        batch = guide->cfg.batch;
+        if (batch > (1u << 24) / kRecBatches)
+            return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "guide batch must be at most 2^22 records");
+        rec_cap = kRecBatches * batch;
+        void* gm;
+        const size_t gbytes = 2 * cap * sizeof(uint4) + cap * (3 * sizeof(float4) + 40 * sizeof(float) + sizeof(uint32_t)) +
+                              static_cast<size_t>(rec_cap) * 6 * sizeof(float4) + 1024;
+        if ((st = scratch(ctx, 2, gbytes, &gm)) != SPT_OK) return st;
+        char* g = static_cast<char*>(gm);
+        A.r = reinterpret_cast<uint4*>(g);
+        B.r = A.r + cap;
+        G.infer_in = reinterpret_cast<float4*>(B.r + cap);
+        G.lobes = reinterpret_cast<float*>(G.infer_in + 3 * cap);
+        G.slot_list = reinterpret_cast<uint32_t*>(G.lobes + 40 * cap);
+        G.rec = reinterpret_cast<float4*>(reinterpret_cast<char*>(G.slot_list + cap) + 256 -
+                                          (reinterpret_cast<uintptr_t>(G.slot_list + cap) & 255));
+        G.recx = G.rec + 4ull * rec_cap;
+        G.mix = guide->cfg.mix;
+        G.rec_cap = rec_cap;
+        const uint32_t on = train_budget > 0 ? 1u : 0u;
+        SPT_CUDA(ctx, cudaMemcpyAsync(&d_ctr->train_on, &on, sizeof(on), cudaMemcpyHostToDevice, ctx->stream));
+        SPT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    Counters* h_ctr;
+    if ((st = pinned(ctx, sizeof(Counters), reinterpret_cast<void**>(&h_ctr))) != SPT_OK) return st;
+    Wave W{d_jobs, static_cast<uint32_t>(jobs.size()), total, static_cast<uint32_t>(cap)};
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    const unsigned eb = tune.extend_block ? tune.extend_block : 128, sb = tune.shade_block ? tune.shade_block : 128;
+    const unsigned g_gen = static_cast<unsigned>(std::min<uint64_t>((cap + 255) / 256, 8ull * sms));
+    const unsigned g_ext = static_cast<unsigned>(std::min<uint64_t>((cap + eb - 1) / eb, 16ull * sms * 128 / eb));
+    const unsigned g_shd = static_cast<unsigned>(std::min<uint64_t>((cap + sb - 1) / sb, 16ull * sms * 128 / sb));
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extend_df, 128, 0);
+    const unsigned g_df = static_cast<unsigned>(sms * std::max(1, per_sm));
+    // one CUDA graph = two iterations (A -> B, B -> A)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    SPT_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    for (int it = 0; it < 2; ++it) {
+        PathBuf& cur = it ? B : A;
+        PathBuf& nxt = it ? A : B;
+        k_generate<<<g_gen, 256, 0, ctx->stream>>>(W, d_ctr, cur);
+        if (trav == 2) k_extend_df<<<g_df, 128, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
+        else if (trav == 1) k_extend<1><<<g_ext, eb, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
+        else k_extend<0><<<g_ext, eb, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
+        if (guide) {
+            k_guide_collect<<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, hits, G);
+            guide->infer_list(G.infer_in, &d_ctr->n_guided, static_cast<uint32_t>(cap), G.lobes, ctx->stream);
+            k_shade<true><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G);
+        } else {
+            k_shade<false><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G);
+        }
+        k_advance<<<1, 1, 0, ctx->stream>>>(W, d_ctr);
+    }
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaStreamEndCapture");
+    ce = cudaGraphInstantiate(&exec, graph, 0);
+    if (ce != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return cuda_fail(ctx, ce, "cudaGraphInstantiate");
+    }
+    SPT_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    // Bounded loop: a path lives at most ~1001 bounces (the roulette cap), plus one iteration per pool
+    // refill; the counter check ends it as soon as all paths are done.
+    const uint64_t max_iter = (total / cap + 2) * 1100ull;
+    const unsigned check = std::max(1u, tune.check_every / 2);
+    uint64_t it = 0;
+    bool done = false;
+    bool training = guide && train_budget > 0, pending = false;
+    uint32_t steps = 0;
+    // Optimiser steps on the n records in the buffer, batch records per step (the last step takes
+    // the remainder), then a fresh generation of records.
+    auto train = [&](uint32_t n) -> spt_status {
+        k_record_weights<<<256, 256, 0, ctx->stream>>>(G.rec, G.recx, n);
+        for (uint32_t off = 0; off < n && steps < train_budget; off += batch) {
+            const uint32_t m = std::min(batch, n - off);
+            if (m < batch / 4 && off > 0) break;   // too few records left for a step of its own
+            spt_status s2 = guide->step(G.rec + 4ull * off, m, nullptr);
+            if (s2 != SPT_OK) return s2;
+            ++steps;
+        }
+        training = steps < train_budget;
+        k_next_generation<<<1, 1, 0, ctx->stream>>>(d_ctr, training ? 1u : 0u);
+        return SPT_OK;
+    };
+    st = SPT_OK;
+    while (!done) {
+        for (unsigned k = 0; k < check; ++k, it += 2) {
+            ce = cudaGraphLaunch(exec, ctx->stream);
+            if (ce != cudaSuccess) break;
+        }
+        if (ce != cudaSuccess) {
+            st = cuda_fail(ctx, ce, "cudaGraphLaunch");
+            break;
+        }
+        ce = cudaMemcpyAsync(h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+        if (ce != cudaSuccess) {
+            st = cuda_fail(ctx, ce, "path tracer iteration");
+            break;
+        }
+        done = h_ctr->next_path >= total && h_ctr->n_alive == 0;
+        const uint32_t n_rec = std::min(h_ctr->rec_count, rec_cap);
+        if (training && done) {
+            // every path has ended: all records carry their final radiance
+            if (n_rec >= std::min(batch, 1024u) && (st = train(n_rec)) != SPT_OK) break;
+        } else if (training && n_rec >= rec_cap) {
+            // A full record buffer takes no more records; its paths keep adding the radiance they
+            // find.  The steps wait one check interval (check_every bounces) so most of it is in.
+            if (!pending) {
+                pending = true;
+            } else {
+                pending = false;
+                if ((st = train(n_rec)) != SPT_OK) break;
+            }
+        }
+        if (!done && it > max_iter) {
+            st = fail(ctx, SPT_ERR_TIMEOUT, "path tracer did not finish its bounded loop");
+            break;
+        }
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (train_steps) *train_steps = steps;
+    if (st != SPT_OK) return st;
+    for (const PtJob& J : jobs) {
+        if (J.s_end != J.spp) continue;
+        const uint64_t img_elems = 3ull * J.cam.width * J.cam.height;
+        k_finalize<<<static_cast<unsigned>(std::min<uint64_t>((img_elems + 255) / 256, 4096)), 256, 0, ctx->stream>>>(
+            J.image, img_elems, 1.0f / static_cast<float>(J.spp));
+    }
+    SPT_CUDA(ctx, cudaGetLastError());
+    SPT_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    st = check_status(ctx);
+    if (st != SPT_OK) return st;
+    *segments = h_ctr->segments;
+    SPT_CUDA(ctx, cudaEventElapsedTime(gpu_ms, ctx->ev0, ctx->ev1));
+    return SPT_OK;
+}
+
 }  // namespace spt
 
 using namespace spt;
@@ -219,95 +667,18 @@ namespace {
 
 spt_status pathtrace_impl(spt_context* ctx, const spt_scene* sc, const spt_camera* cam, const spt_pt_params* p,
                           float* d_image, spt_render_stats* stats) {
-    if (!ctx || !sc || !p || !d_image) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (p->pixel_sampler < SPT_PIXEL_UNIFORM || p->pixel_sampler > SPT_PIXEL_JITTERED)
-        return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "unknown pixel sampler");
-    if (p->termination != SPT_TERMINATE_MAX_DEPTH && p->termination != SPT_TERMINATE_RUSSIAN_ROULETTE)
-        return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "unknown path termination criterion");
-    if (p->spp == 0) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "spp must be > 0");
-    if (p->path_length < 0 || p->max_depth < 0) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "negative path length");
-    SPT_CUDA(ctx, cudaSetDevice(ctx->device));
-    PtConst C;
-    std::memset(&C, 0, sizeof(C));
-    spt_status st = make_camera(ctx, cam, C.cam);
+    if (!ctx) return SPT_ERR_INVALID_ARGUMENT;
+    std::vector<PtJob> jobs(1);
+    spt_status st = make_job(ctx, sc, cam, p, d_image, jobs[0]);
     if (st != SPT_OK) return st;
-    C.S = sc->dev;
-    C.seed = p->seed;
-    C.sampler = p->pixel_sampler;
-    C.spp = p->spp;
-    C.nsub = 1;
-    C.sw = 1.0f;
-    if (p->pixel_sampler != SPT_PIXEL_UNIFORM) {  // regular/jittered round spp up to a square
-        C.nsub = static_cast<uint32_t>(std::ceil(std::sqrt(static_cast<double>(p->spp))));
-        C.spp = C.nsub * C.nsub;
-        C.sw = 1.0f / C.nsub;
-    }
-    C.rr = p->termination == SPT_TERMINATE_RUSSIAN_ROULETTE;
-    C.path_length = p->path_length;
-    C.cap = p->max_depth > 0 ? p->max_depth - 1 : 1000;
-    C.npix = C.cam.vp_width * C.cam.vp_height;
-    C.spp_offset = p->spp_offset;
-    C.total = static_cast<uint64_t>(C.npix) * C.spp;
-    C.image = d_image;
-    const uint64_t img_elems = 3ull * C.cam.width * C.cam.height;
-    SPT_CUDA(ctx, cudaMemsetAsync(d_image, 0, img_elems * sizeof(float), ctx->stream));
-    if (C.total == 0 || (!C.rr && C.path_length <= 0)) {
-        if (stats) std::memset(stats, 0, sizeof(*stats));
-        return check_status(ctx);
-    }
-    uint64_t cap = std::min<uint64_t>(C.total, 1ull << 21);
-    C.capacity = static_cast<uint32_t>(cap);
-    // scratch: 2 path buffers (4 float4 each) + hits + counters
-    void* mem;
-    const size_t buf_bytes = cap * sizeof(float4);
-    if ((st = scratch(ctx, 5, buf_bytes * 9 + sizeof(Counters) + 256, &mem)) != SPT_OK) return st;
-    char* base = static_cast<char*>(mem);
-    PathBuf A{reinterpret_cast<float4*>(base), reinterpret_cast<float4*>(base + buf_bytes),
-              reinterpret_cast<float4*>(base + 2 * buf_bytes), reinterpret_cast<float4*>(base + 3 * buf_bytes)};
-    PathBuf B{reinterpret_cast<float4*>(base + 4 * buf_bytes), reinterpret_cast<float4*>(base + 5 * buf_bytes),
-              reinterpret_cast<float4*>(base + 6 * buf_bytes), reinterpret_cast<float4*>(base + 7 * buf_bytes)};
-    float4* hits = reinterpret_cast<float4*>(base + 8 * buf_bytes);
-    Counters* d_ctr = reinterpret_cast<Counters*>(base + 9 * buf_bytes);
-    SPT_CUDA(ctx, cudaMemsetAsync(d_ctr, 0, sizeof(Counters), ctx->stream));
-    Counters* h_ctr;
-    if ((st = pinned(ctx, sizeof(Counters), reinterpret_cast<void**>(&h_ctr))) != SPT_OK) return st;
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-    const unsigned g_gen = static_cast<unsigned>(std::min<uint64_t>((cap + 255) / 256, 8ull * sms));
-    const unsigned g_ext = static_cast<unsigned>(std::min<uint64_t>((cap + 127) / 128, 16ull * sms));
-    SPT_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    // Bounded loop: a path can live at most 1001 bounces (the roulette cap), plus one iteration
-    // per pool refill; the check below ends it as soon as all paths are done.
-    const uint64_t max_iter = (C.total / cap + 2) * 1100ull;
-    uint64_t it = 0;
-    bool done = false;
-    while (!done) {
-        for (int k = 0; k < 8; ++k, ++it) {
-            PathBuf& cur = (it & 1) ? B : A;
-            PathBuf& nxt = (it & 1) ? A : B;
-            k_generate<<<g_gen, 256, 0, ctx->stream>>>(C, d_ctr, cur);
-            k_extend<<<g_ext, 128, 0, ctx->stream>>>(C, d_ctr, cur, hits, ctx->d_status);
-            k_shade<<<g_ext, 128, 0, ctx->stream>>>(C, d_ctr, cur, nxt, hits);
-            k_advance<<<1, 1, 0, ctx->stream>>>(C, d_ctr);
-        }
-        SPT_CUDA(ctx, cudaGetLastError());
-        SPT_CUDA(ctx, cudaMemcpyAsync(h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
-        SPT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        done = h_ctr->next_path >= C.total && h_ctr->n_alive == 0;
-        if (!done && it > max_iter) return fail(ctx, SPT_ERR_TIMEOUT, "path tracer did not finish its bounded loop");
-    }
-    k_finalize<<<static_cast<unsigned>(std::min<uint64_t>((img_elems + 255) / 256, 4096)), 256, 0, ctx->stream>>>(
-        d_image, img_elems, 1.0f / static_cast<float>(C.spp));
-    SPT_CUDA(ctx, cudaGetLastError());
-    SPT_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
-    st = check_status(ctx);
+    uint64_t segs = 0;
+    float ms = 0.0f;
+    st = render_jobs(ctx, jobs, default_tune(), &segs, &ms);
     if (st != SPT_OK) return st;
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
-        stats->paths = C.total;
-        stats->segments = h_ctr->segments;
-        float ms = 0.0f;
-        SPT_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        stats->paths = jobs[0].total;
+        stats->segments = segs;
         stats->gpu_ms = ms;
     }
     return SPT_OK;

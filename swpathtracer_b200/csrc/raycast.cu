@@ -9,19 +9,41 @@
 #include <limits>
 
 #include "spt_internal.h"
-#include "traverse.cuh"
+#include "traverse_wide.cuh"
 
 namespace spt {
 namespace {
 
 constexpr int kBlock = 128;
 
+// Persistent variant: wide traversal, lanes refilled from a global ray counter (traverse_wide.cuh).
+__global__ void __launch_bounds__(kBlock) k_intersect_df(DevScene S, const float4* __restrict__ rays, uint64_t n,
+                                                         spt_hit* __restrict__ hits, uint32_t* status,
+                                                         unsigned long long* next) {
+    persistent_trace(
+        S, n, next, status,
+        [&](uint64_t i, V3& o, V3& d) {
+            const float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+            o = f3v(a);
+            d = f3v(b);
+        },
+        [&](uint64_t i, const Hit1& h) {
+            spt_hit out;
+            out.t = h.t;
+            out.prim_id = h.found ? slot_prim(S, h.slot) : SPT_MISS;
+            out.u = h.u;
+            out.v = h.v;
+            hits[i] = out;
+        });
+}
+
+template <int TRAV>
 __global__ void __launch_bounds__(kBlock) k_intersect(DevScene S, const float4* __restrict__ rays, uint64_t n,
                                                       spt_hit* __restrict__ hits, uint32_t* status) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
-    Hit1 h = closest_hit<kStack>(S, f3v(a), f3v(b), status);
+    Hit1 h = trace_closest<TRAV>(S, f3v(a), f3v(b), status);
     spt_hit o;
     o.t = h.t;
     o.prim_id = h.found ? slot_prim(S, h.slot) : SPT_MISS;
@@ -87,7 +109,7 @@ __device__ __forceinline__ void tile_pixel(uint32_t& x, uint32_t& y) {
     y = blockIdx.y * 16 + (w >> 1) * 4 + (lane >> 3);
 }
 
-template <int MODE>
+template <int MODE, int TRAV>
 __global__ void __launch_bounds__(256) k_raycast(DevScene S, DevCamera cam, void* __restrict__ out,
                                                  StatAcc* stats, uint32_t* status) {
     uint32_t x, y;
@@ -117,7 +139,7 @@ __global__ void __launch_bounds__(256) k_raycast(DevScene S, DevCamera cam, void
                 q[0] = nrm.x; q[1] = nrm.y; q[2] = nrm.z;
             }
         } else {
-            Hit1 h = closest_hit<kStack>(S, o, d, status);
+            Hit1 h = trace_closest<TRAV>(S, o, d, status);
             if (MODE == SPT_RAYCAST_DEPTH) {
                 static_cast<float*>(out)[idx] = h.found ? h.t : -1.0f;
             } else {
@@ -142,8 +164,20 @@ spt_status launch_intersect(spt_context* ctx, const spt_scene* sc, const float* 
                             cudaStream_t s) {
     if (n == 0) return SPT_OK;
     if (n > (1ull << 36)) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "too many rays in one call");
-    k_intersect<<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n, d_hits,
-                                                         ctx->d_status);
+    if (sc->dev.traversal == 2) {
+        unsigned long long* next = nullptr;
+        spt_status st = fetch_counter(ctx, s, &next);
+        if (st != SPT_OK) return st;
+        static int grid = 0;
+        if (!grid) grid = persistent_grid(ctx, reinterpret_cast<const void*>(k_intersect_df), kBlock);
+        k_intersect_df<<<grid, kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n, d_hits,
+                                              ctx->d_status, next);
+    } else if (sc->dev.traversal == 1)
+        k_intersect<1><<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n,
+                                                                d_hits, ctx->d_status);
+    else
+        k_intersect<0><<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n,
+                                                                d_hits, ctx->d_status);
     SPT_CUDA(ctx, cudaGetLastError());
     return SPT_OK;
 }
@@ -161,12 +195,16 @@ spt_status launch_count(spt_context* ctx, const spt_scene* sc, const float* d_ra
 static spt_status launch_raycast(spt_context* ctx, const spt_scene* sc, const DevCamera& cam, int32_t mode, void* d_out,
                                  StatAcc* d_stats, cudaStream_t s) {
     dim3 grid((cam.width + 15) / 16, (cam.height + 15) / 16);
-    if (mode == SPT_RAYCAST_NORMAL)
-        k_raycast<SPT_RAYCAST_NORMAL><<<grid, 256, 0, s>>>(sc->dev, cam, d_out, d_stats, ctx->d_status);
-    else if (mode == SPT_RAYCAST_DEPTH)
-        k_raycast<SPT_RAYCAST_DEPTH><<<grid, 256, 0, s>>>(sc->dev, cam, d_out, d_stats, ctx->d_status);
-    else
-        k_raycast<SPT_RAYCAST_COUNT><<<grid, 256, 0, s>>>(sc->dev, cam, d_out, d_stats, ctx->d_status);
+    const bool w = sc->dev.traversal >= 1;
+    if (mode == SPT_RAYCAST_NORMAL) {
+        if (w) k_raycast<SPT_RAYCAST_NORMAL, 1><<<grid, 256, 0, s>>>(sc->dev, cam, d_out, d_stats, ctx->d_status);
+        else k_raycast<SPT_RAYCAST_NORMAL, 0><<<grid, 256, 0, s>>>(sc->dev, cam, d_out, d_stats, ctx->d_status);
+    } else if (mode == SPT_RAYCAST_DEPTH) {
+        if (w) k_raycast<SPT_RAYCAST_DEPTH, 1><<<grid, 256, 0, s>>>(sc->dev, cam, d_out, d_stats, ctx->d_status);
+        else k_raycast<SPT_RAYCAST_DEPTH, 0><<<grid, 256, 0, s>>>(sc->dev, cam, d_out, d_stats, ctx->d_status);
+    } else {
+        k_raycast<SPT_RAYCAST_COUNT, 0><<<grid, 256, 0, s>>>(sc->dev, cam, d_out, d_stats, ctx->d_status);
+    }
     SPT_CUDA(ctx, cudaGetLastError());
     return SPT_OK;
 }

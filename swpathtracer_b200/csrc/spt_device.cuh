@@ -53,13 +53,16 @@ struct DevScene {
     const DevBsdf* bsdf;
     const DevMaterial* mat;
     const int* layer_ids;
+    const uint4* wnode;         // 8-wide quantized nodes, 5 x uint4 each (wide_build.h)
+    const float4* wtri;         // 3 float4 per triangle in wide-node order: {v0, rank}{e1, type}{e2, leaf}
     float root_min[3], root_max[3];
     float bg[3];
-    uint32_t n_prims, n_inner, n_leaves, n_nodes2;
+    uint32_t n_prims, n_inner, n_leaves, n_nodes2, n_wnodes;
     int root_is_leaf;           // the whole scene is one leaf (or no acceleration structure)
     int no_accel;               // NoAccelStructure semantics (no_accel_structure.cpp:9-30)
     int has_spheres;
     int empty;
+    int traversal;              // 0: binary pair nodes, 1: 8-wide quantized nodes, 2: 1 + dynamic fetch
 };
 
 // Camera constants computed on the host exactly as the reference constructors do.

@@ -26,6 +26,9 @@ struct spt_context {
     size_t scratch_bytes[8] = {};
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // ray counters of the persistent (dynamic-fetch) kernels: a ring, one slot per launch
+    unsigned long long* d_fetch = nullptr;
+    uint32_t fetch_slot = 0;
 };
 
 struct spt_scene {
@@ -67,5 +70,11 @@ spt_status launch_count(spt_context* ctx, const spt_scene* sc, const float* d_ra
                         uint32_t* d_tests, uint32_t* d_hits, uint32_t* d_prim_tests, cudaStream_t s);
 
 constexpr int kStack = 64;
+constexpr uint32_t kFetchRing = 1024;
+
+// Zeroes the next counter of the ring on stream s and returns it (persistent kernels).
+spt_status fetch_counter(spt_context* ctx, cudaStream_t s, unsigned long long** out);
+// Blocks of `block` threads that fill every SM once for `kernel` (persistent launches).
+int persistent_grid(spt_context* ctx, const void* kernel, int block);
 
 }  // namespace spt

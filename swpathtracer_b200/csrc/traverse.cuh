@@ -25,6 +25,7 @@ __device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
 struct Hit1 {
     float t, u, v;
     uint32_t slot;
+    uint32_t leaf;   // reference leaf of the hit (wide traversal), for the deferred inside test
     bool found;
 };
 
@@ -52,6 +53,7 @@ __device__ __forceinline__ Hit1 closest_hit(const DevScene& S, V3 o, V3 d, uint3
     h.t = inf_f();
     h.u = h.v = 0.0f;
     h.slot = 0;
+    h.leaf = 0;
     h.found = false;
     if (S.empty) return h;
     if (S.no_accel) {  // NoAccelStructure::intersect: every primitive, no box test, strict <
@@ -134,6 +136,7 @@ __device__ __forceinline__ Hit1 count_traverse(const DevScene& S, V3 o, V3 d, Co
     h.t = inf_f();
     h.u = h.v = 0.0f;
     h.slot = 0;
+    h.leaf = 0;
     h.found = false;
     c.tests = c.hits = c.prim_tests = 0;
     if (S.empty) return h;

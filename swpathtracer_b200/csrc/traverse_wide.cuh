@@ -1,0 +1,335 @@
+// traverse_wide.cuh -- closest hit over the 8-wide quantized BVH (wide_build.h).
+//
+// Why the answer is still the reference's: every box of the reference tree below the root is its
+// primitives' bounds inflated by 1e-3 (acceleration/sbvh.cpp:409-412), and the wide nodes' boxes
+// contain those boxes (quantized outward).  A hit the reference keeps lies inside its leaf box
+// (inside() below), hence at least ~1e-3 inside every ancestor box, so a conservative box test --
+// here one FMA per plane on the quantized grid, with the interval clipped to [0, best t] -- can only
+// visit more nodes than needed, never skip the node holding that hit.  The root box is tested with the
+// reference's own slab test first, and every candidate is accepted by the reference's exact rules:
+// Moller-Trumbore as in triangle.cpp, t > 0, the hit point inside the reference leaf box (+-1e-3), and
+// the smallest (t, rank) with rank = the reference's depth-first leaf order.
+#pragma once
+
+#include "spt_internal.h"
+#include "traverse.cuh"
+
+namespace spt {
+
+constexpr int kWideStack = 32;
+
+__device__ __forceinline__ uint32_t byte_of(uint32_t lo, uint32_t hi, int j) {
+    return ((j < 4 ? lo : hi) >> (8 * (j & 3))) & 0xFFu;
+}
+
+__device__ __forceinline__ float exp2i(int e) { return __int_as_float((e + 127) << 23); }
+
+struct WideRay {
+    V3 o;
+    float ix, iy, iz;   // 1/d with zero components replaced by a tiny signed value
+    uint32_t inv_oct;   // slot order key: slot ^ inv_oct, ascending = near to far
+    const uint4* top;   // the first n_top nodes staged in shared memory by the block, or null
+    uint32_t n_top;
+};
+
+// Nodes staged in shared memory: the top levels of the breadth-first node order, which every ray
+// from the root visits.
+constexpr uint32_t kTopNodes = 96;
+
+__device__ __forceinline__ void stage_top_nodes(const DevScene& S, uint4* smem, uint32_t& n_top) {
+    n_top = S.n_wnodes < kTopNodes ? S.n_wnodes : kTopNodes;
+    for (uint32_t i = threadIdx.x; i < 5 * n_top; i += blockDim.x) smem[i] = __ldg(S.wnode + i);
+    __syncthreads();
+}
+
+__device__ __forceinline__ float safe_inv(float d) {
+    return 1.0f / (fabsf(d) > 1e-20f ? d : copysignf(1e-20f, d));
+}
+
+__device__ __forceinline__ void wide_node_hits(const DevScene& S, const WideRay& r, uint32_t idx, float best_t,
+                                               uint32_t& g_base, uint32_t& g_hits, uint32_t& g_imask,
+                                               uint32_t& t_base, uint32_t& t_mask) {
+    uint4 w0, w1, w2, w3, w4;
+    if (idx < r.n_top) {
+        const uint4* n = r.top + 5 * idx;
+        w0 = n[0]; w1 = n[1]; w2 = n[2]; w3 = n[3]; w4 = n[4];
+    } else {
+        const uint4* n = S.wnode + 5 * idx;
+        w0 = __ldg(n); w1 = __ldg(n + 1); w2 = __ldg(n + 2); w3 = __ldg(n + 3); w4 = __ldg(n + 4);
+    }
+    const int ex = static_cast<int8_t>(w0.w & 0xFFu), ey = static_cast<int8_t>((w0.w >> 8) & 0xFFu),
+              ez = static_cast<int8_t>((w0.w >> 16) & 0xFFu);
+    const uint32_t imask = w0.w >> 24;
+    const float sx = exp2i(ex) * r.ix, sy = exp2i(ey) * r.iy, sz = exp2i(ez) * r.iz;
+    const float ox = (__uint_as_float(w0.x) - r.o.x) * r.ix;
+    const float oy = (__uint_as_float(w0.y) - r.o.y) * r.iy;
+    const float oz = (__uint_as_float(w0.z) - r.o.z) * r.iz;
+    // the near plane is the low plane when 1/d >= 0
+    const bool nx = r.ix >= 0.0f, ny = r.iy >= 0.0f, nz = r.iz >= 0.0f;
+    uint32_t hits = 0, tm = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const uint32_t meta = byte_of(w1.z, w1.w, j);
+        const bool inner = (imask >> j) & 1u;
+        const float lx = static_cast<float>(byte_of(w2.x, w2.y, j)), ly = static_cast<float>(byte_of(w2.z, w2.w, j));
+        const float lz = static_cast<float>(byte_of(w3.x, w3.y, j)), hx = static_cast<float>(byte_of(w3.z, w3.w, j));
+        const float hy = static_cast<float>(byte_of(w4.x, w4.y, j)), hz = static_cast<float>(byte_of(w4.z, w4.w, j));
+        const float tnx = __fmaf_rn(nx ? lx : hx, sx, ox), tfx = __fmaf_rn(nx ? hx : lx, sx, ox);
+        const float tny = __fmaf_rn(ny ? ly : hy, sy, oy), tfy = __fmaf_rn(ny ? hy : ly, sy, oy);
+        const float tnz = __fmaf_rn(nz ? lz : hz, sz, oz), tfz = __fmaf_rn(nz ? hz : lz, sz, oz);
+        const float tmin = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+        const float tmax = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
+        const bool hit = (inner || meta != 0u) && tmin <= tmax;
+        if (hit) {
+            if (inner) hits |= 1u << (j ^ r.inv_oct);
+            else tm |= (meta >> 5) << (meta & 31u);
+        }
+    }
+    g_base = w1.x;
+    g_hits = hits;
+    g_imask = imask;
+    t_base = w1.y;
+    t_mask = tm;
+}
+
+// One candidate triangle/sphere.  Without `exact`, the reference's inside-the-leaf-box test is
+// deferred to the final hit (WideTraversal::finish / closest_hit_wide): a candidate that beats the
+// current best on (t, rank) is kept either way, and if the final hit fails the test the ray is traced
+// again with the test applied to every candidate.  Pruning with a best t that might later be rejected
+// is safe because the final best, once it passes, is the minimum over all candidates with t > 0.
+__device__ __forceinline__ void wide_candidate(const DevScene& S, uint32_t wslot, V3 o, V3 d, Hit1& h, bool exact) {
+    const float4 a = __ldg(S.wtri + 3 * wslot);
+    const float4 b = __ldg(S.wtri + 3 * wslot + 1);
+    const float4 c = __ldg(S.wtri + 3 * wslot + 2);
+    const uint32_t rank = __float_as_uint(a.w);
+    float t, u = 0.0f, v = 0.0f;
+    const bool sphere = __float_as_int(b.w) == SPT_PRIM_SPHERE;
+    const bool ok = sphere ? sphere_test(f3v(a), c.x, o, d, t) : tri_test(f3v(a), f3v(b), f3v(c), o, d, t, u, v);
+    if (!ok || !(t > 0.0f)) return;
+    if (!(t < h.t || (h.found && t == h.t && rank < h.slot))) return;
+    const uint32_t leaf = __float_as_uint(c.w);
+    if (exact && !inside(S.leaf_box + 6 * leaf, hit_pos(sphere, o, d, t))) return;
+    h.t = t;
+    h.u = u;
+    h.v = v;
+    h.slot = rank;
+    h.leaf = leaf;
+    h.found = true;
+}
+
+// The deferred inside test of the final hit (o + d*t is the same float expression for both
+// primitive kinds).
+__device__ __forceinline__ bool final_inside(const DevScene& S, const Hit1& h, V3 o, V3 d) {
+    return !h.found || inside(S.leaf_box + 6 * h.leaf, o + d * h.t);
+}
+
+__device__ __forceinline__ Hit1 closest_hit_wide_pass(const DevScene& S, V3 o, V3 d, uint32_t* overflow, bool exact) {
+    Hit1 h;
+    h.t = inf_f();
+    h.u = h.v = 0.0f;
+    h.slot = 0;
+    h.leaf = 0;
+    h.found = false;
+    if (S.empty) return h;
+    if (S.no_accel) {
+        for (uint32_t s = 0; s < S.n_prims; ++s) prim_candidate(S, s, nullptr, o, d, false, h);
+        return h;
+    }
+    {
+        const RayInv ri = ray_inv(o, d);
+        float t0, t1;
+        if (!slab(ri, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], t0,
+                  t1))
+            return h;
+    }
+    WideRay r;
+    r.o = o;
+    r.ix = safe_inv(d.x);
+    r.iy = safe_inv(d.y);
+    r.iz = safe_inv(d.z);
+    r.inv_oct = (r.ix >= 0.0f ? 0u : 1u) | (r.iy >= 0.0f ? 0u : 2u) | (r.iz >= 0.0f ? 0u : 4u);
+    r.top = nullptr;
+    r.n_top = 0;
+    uint2 stack[kWideStack];
+    int sp = 0;
+    uint32_t g_base, g_hits, g_imask, t_base, t_mask;
+    wide_node_hits(S, r, 0, h.t, g_base, g_hits, g_imask, t_base, t_mask);
+    for (;;) {
+        while (t_mask) {
+            const int k = __ffs(t_mask) - 1;
+            t_mask &= t_mask - 1;
+            wide_candidate(S, t_base + k, o, d, h, exact);
+        }
+        if (!g_hits) {
+            if (sp == 0) break;
+            --sp;
+            g_base = stack[sp].x;
+            g_hits = stack[sp].y & 0xFFu;
+            g_imask = stack[sp].y >> 8;
+        }
+        const uint32_t key = __ffs(g_hits) - 1;
+        g_hits &= g_hits - 1;
+        const uint32_t s = key ^ r.inv_oct;
+        const uint32_t child = g_base + __popc(g_imask & ((1u << s) - 1u));
+        if (g_hits) {
+            if (sp < kWideStack) {
+                stack[sp] = make_uint2(g_base, g_hits | (g_imask << 8));
+                ++sp;
+            } else {
+                atomicOr(overflow, 1u);
+            }
+        }
+        wide_node_hits(S, r, child, h.t, g_base, g_hits, g_imask, t_base, t_mask);
+    }
+    return h;
+}
+
+__device__ __forceinline__ Hit1 closest_hit_wide(const DevScene& S, V3 o, V3 d, uint32_t* overflow) {
+    Hit1 h = closest_hit_wide_pass(S, o, d, overflow, false);
+    if (!final_inside(S, h, o, d)) h = closest_hit_wide_pass(S, o, d, overflow, true);
+    return h;
+}
+
+// The same traversal as a resumable state, one node (and its triangles) per step, for kernels that
+// keep a warp's lanes busy by giving a lane a new ray as soon as its ray is finished.
+struct WideTraversal {
+    V3 o, d;
+    WideRay r;
+    Hit1 h;
+    uint2 stack[kWideStack];
+    int sp;
+    uint32_t g_base, g_hits, g_imask, t_base, t_mask;
+    bool exact;
+    const uint4* top = nullptr;   // shared-memory copy of the top nodes (set by the kernel)
+    uint32_t n_top = 0;
+
+    // Returns false when the ray is already finished (empty scene or root box missed).
+    __device__ __forceinline__ bool start(const DevScene& S, V3 o_, V3 d_, bool exact_ = false) {
+        o = o_;
+        d = d_;
+        exact = exact_;
+        h.t = inf_f();
+        h.u = h.v = 0.0f;
+        h.slot = 0;
+        h.leaf = 0;
+        h.found = false;
+        sp = 0;
+        if (S.empty) return false;
+        const RayInv ri = ray_inv(o, d);
+        float t0, t1;
+        if (!slab(ri, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], t0, t1))
+            return false;
+        r.o = o;
+        r.ix = safe_inv(d.x);
+        r.iy = safe_inv(d.y);
+        r.iz = safe_inv(d.z);
+        r.inv_oct = (r.ix >= 0.0f ? 0u : 1u) | (r.iy >= 0.0f ? 0u : 2u) | (r.iz >= 0.0f ? 0u : 4u);
+        r.top = top;
+        r.n_top = n_top;
+        wide_node_hits(S, r, 0, h.t, g_base, g_hits, g_imask, t_base, t_mask);
+        return true;
+    }
+
+    // One step: the pending triangles, then the next node.  Returns false once the ray is done.
+    __device__ __forceinline__ bool step(const DevScene& S, uint32_t* overflow) {
+        while (t_mask) {
+            const int k = __ffs(t_mask) - 1;
+            t_mask &= t_mask - 1;
+            wide_candidate(S, t_base + k, o, d, h, exact);
+        }
+        if (!g_hits) {
+            if (sp == 0) return false;
+            --sp;
+            g_base = stack[sp].x;
+            g_hits = stack[sp].y & 0xFFu;
+            g_imask = stack[sp].y >> 8;
+        }
+        const uint32_t key = __ffs(g_hits) - 1;
+        g_hits &= g_hits - 1;
+        const uint32_t s = key ^ r.inv_oct;
+        const uint32_t child = g_base + __popc(g_imask & ((1u << s) - 1u));
+        if (g_hits) {
+            if (sp < kWideStack) {
+                stack[sp] = make_uint2(g_base, g_hits | (g_imask << 8));
+                ++sp;
+            } else {
+                atomicOr(overflow, 1u);
+            }
+        }
+        wide_node_hits(S, r, child, h.t, g_base, g_hits, g_imask, t_base, t_mask);
+        return true;
+    }
+
+    // After step() returned false: true if the result is final; false if the final hit failed the
+    // deferred inside test and the traversal restarted in exact mode (keep stepping).
+    __device__ __forceinline__ bool finish(const DevScene& S) {
+        if (exact || final_inside(S, h, o, d)) return true;
+        start(S, o, d, true);
+        return false;
+    }
+};
+
+// Persistent warps with dynamic ray fetch (after Aila & Laine, "Understanding the Efficiency of Ray
+// Traversal on GPUs", HPG 2009): a lane whose ray is finished takes the next ray at once instead of
+// idling until the warp's longest ray ends.  Ray indices come from a warp-local pool refilled
+// kChunk at a time from one global counter, so the counter sees one atomic per kChunk rays.
+// load(i, o, d) fetches ray i; store(i, h) writes its result.
+constexpr uint32_t kChunk = 256;
+
+template <typename Load, typename Store>
+__device__ __forceinline__ void persistent_trace(const DevScene& S, uint64_t n, unsigned long long* next,
+                                                 uint32_t* overflow, Load load, Store store) {
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    __shared__ uint4 top[5 * kTopNodes];
+    WideTraversal tr;
+    stage_top_nodes(S, top, tr.n_top);
+    tr.top = top;
+    bool active = false, exhausted = false;
+    uint64_t mine = 0;
+    unsigned long long pool = 0, pool_end = 0;  // warp-uniform
+    for (;;) {
+        const unsigned need = __ballot_sync(0xFFFFFFFFu, !active && !exhausted);
+        if (need) {
+            const uint32_t cnt = __popc(need), rank = __popc(need & lt);
+            const unsigned long long have = pool_end - pool;
+            unsigned long long fresh = 0;
+            if (have < cnt) {
+                if (lane == 0) fresh = atomicAdd(next, static_cast<unsigned long long>(kChunk));
+                fresh = __shfl_sync(0xFFFFFFFFu, fresh, 0);
+            }
+            if (!active && !exhausted) {
+                mine = rank < have ? pool + rank : fresh + (rank - have);
+                if (mine >= n) {
+                    exhausted = true;
+                } else {
+                    V3 o, d;
+                    load(mine, o, d);
+                    active = tr.start(S, o, d);
+                    if (!active) store(mine, tr.h);
+                }
+            }
+            if (have < cnt) {
+                pool = fresh + (cnt - have);
+                pool_end = fresh + kChunk;
+            } else {
+                pool += cnt;
+            }
+        }
+        if (__all_sync(0xFFFFFFFFu, !active && exhausted)) break;
+        if (active && !tr.step(S, overflow) && tr.finish(S)) {
+            store(mine, tr.h);
+            active = false;
+        }
+    }
+}
+
+// Closest hit with the traversal the scene selected (a kernel template parameter, so each kernel
+// carries one traversal's registers).
+template <int TRAV>
+__device__ __forceinline__ Hit1 trace_closest(const DevScene& S, V3 o, V3 d, uint32_t* overflow) {
+    if (TRAV >= 1) return closest_hit_wide(S, o, d, overflow);
+    return closest_hit<kStack>(S, o, d, overflow);
+}
+
+}  // namespace spt

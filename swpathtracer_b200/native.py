@@ -33,6 +33,18 @@ PROTOTYPES = {
     "spt_pathtrace": (i32, [vp, vp, vp, vp, vp, vp]),
     "spt_pathtrace_device": (i32, [vp, vp, vp, vp, vp, vp]),
     "spt_write_ppm": (i32, [C.c_char_p, vp, u32, u32, i32]),
+    "spt_tune_default": (i32, [vp]),
+    "spt_batch_pathtrace": (i32, [vp, vp, u32, vp, vp, vp]),
+    "spt_autotune": (i32, [vp, vp, u32, C.c_char_p, vp]),
+    "spt_guide_create": (i32, [vp, vp, C.POINTER(vp)]),
+    "spt_guide_destroy": (i32, [vp]),
+    "spt_guide_get_params": (i32, [vp, vp, vp]),
+    "spt_guide_set_params": (i32, [vp, vp, vp]),
+    "spt_guide_eval": (i32, [vp, vp, vp, u32, vp]),
+    "spt_guide_gradients": (i32, [vp, vp, vp, u32, vp, vp, vp]),
+    "spt_guide_train": (i32, [vp, vp, vp, u32, vp]),
+    "spt_guide_steps": (i32, [vp, C.POINTER(C.c_uint64)]),
+    "spt_guided_pathtrace_device": (i32, [vp, vp, vp, vp, vp, vp, vp]),
 }
 
 _lib = None

@@ -319,10 +319,10 @@ WALL_COLOURS = [(0.75, 0.75, 0.75), (0.63, 0.06, 0.05), (0.14, 0.45, 0.09)]
 CONDUCTOR_F0 = (0.95, 0.64, 0.54)
 
 
-def _box_into(sb, size):
-    walls, cols, light = open_box(size)
+def _box_into(sb, size, light_size=0.25, emission=15.0):
+    walls, cols, light = open_box(size, light_size)
     wall_mats = [sb.material(sb.layered_bsdf(sb.lambertian(kd=c))) for c in WALL_COLOURS]
-    light_mat = sb.material(sb.layered_bsdf(sb.lambertian(kd=(0.0, 0.0, 0.0))), emission=(15.0, 15.0, 15.0))
+    light_mat = sb.material(sb.layered_bsdf(sb.lambertian(kd=(0.0, 0.0, 0.0))), emission=(emission,) * 3)
     sb.triangles(walls, np.array([wall_mats[c] for c in cols], np.uint32))
     sb.triangles(light, light_mat)
 
@@ -371,6 +371,20 @@ def incoherent_rays(n, seed=1, half_extent=1.5):
     r[:, 5] = s * np.sin(ph)
     r[:, 6] = z
     return r
+
+
+def small_light_box_scene(subdivisions=4, light_size=0.06):
+    """Path guiding workload: the open unit box lit by a small ceiling light of the same power as the
+    box scene's (radiance 15 * (0.25 / light_size)^2), around a Lambertian and a Cook-Torrance
+    sphere.  The path tracer has no light sampling, so a path finds the light only by sampling its
+    direction -- the case a learned directional distribution improves most."""
+    sb = SceneBuilder(background=(0.0, 0.0, 0.0))
+    _box_into(sb, 1.0, light_size=light_size, emission=15.0 * (0.25 / light_size) ** 2)
+    diffuse = sb.material(sb.layered_bsdf(sb.lambertian(kd=(0.8, 0.8, 0.8))))
+    metal = sb.material(sb.layered_bsdf(sb.cook_torrance(roughness=0.3, reflectance_at_normal_incidence=CONDUCTOR_F0)))
+    sb.triangles(displaced_icosphere(subdivisions, radius=0.2, center=(0.3, 0.2, 0.45), amplitude=0.0), diffuse)
+    sb.triangles(displaced_icosphere(subdivisions, radius=0.17, center=(0.72, 0.17, 0.6), amplitude=0.0), metal)
+    return sb
 
 
 def layered_box_scene(subdivisions=8, seed=1):
@@ -435,3 +449,74 @@ def furnace_scene(material="lambertian", reflectance=0.999):
 def furnace_camera(width=64, height=64):
     return camera("orthographic", position=(0, 0, 6), look_at=(0, 0, 0), width=width, height=height,
                   window=(-1.25, 1.25, -1.25, 1.25))
+
+
+def uv_sphere(n_tris, radius=1.0, center=(0.0, 0.0, 0.0), amplitude=0.05, octaves=8, seed=1):
+    """Latitude-longitude sphere with about n_tris triangles (outward winding), radially displaced like
+    displaced_icosphere; float32 [n, 3, 3]."""
+    n_lon = max(3, int(round(np.sqrt(n_tris / 2.0))))
+    n_lat = max(3, int(round(n_tris / (2.0 * n_lon))) + 1)
+    th = np.arange(n_lat + 1) * (np.pi / n_lat)
+    ph = np.arange(n_lon) * (2.0 * np.pi / n_lon)
+    st, ct = np.sin(th), np.cos(th)
+    v = np.stack([np.outer(st, np.cos(ph)), np.repeat(ct[:, None], n_lon, 1), np.outer(st, np.sin(ph))], -1)
+    v = v.reshape(-1, 3)
+    if amplitude != 0.0:
+        v = v * (1.0 + amplitude * fbm(v, octaves=octaves, seed=seed))[:, None]
+    v = v * radius + np.asarray(center, np.float64)[None, :]
+    idx = lambda i, j: i * n_lon + (j % n_lon)
+    faces = []
+    for i in range(n_lat):
+        j = np.arange(n_lon)
+        a, b, c, d = idx(i, j), idx(i, j + 1), idx(i + 1, j), idx(i + 1, j + 1)
+        if i > 0:
+            faces.append(np.stack([a, b, c], 1))
+        if i < n_lat - 1:
+            faces.append(np.stack([b, d, c], 1))
+    f = np.concatenate(faces)
+    tri = v.astype(np.float32)[f]
+    n = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    cen = tri.mean(1) - np.asarray(center, np.float32)
+    flip = (n * cen).sum(1) < 0
+    tri[flip] = tri[flip][:, [0, 2, 1]]
+    return tri
+
+
+def batched_scenes(n=64, seed=2024, min_tris=1000, max_tris=500000, min_res=128, max_res=1024, spp=64,
+                   max_tris_cap=None):
+    """Uneven batch: n seeded scenes, each a displaced sphere of log-uniform [min_tris, max_tris]
+    triangles (radius 0.3) in the open unit box, with a material drawn uniformly from {Lambertian,
+    rough conductor alpha in [0.05, 0.6], smooth dielectric IOR in [1.3, 1.8], layered dielectric over
+    rough conductor}, rendered at a log-uniform square resolution in [min_res, max_res] with `spp`
+    jittered samples, max path length 5.  Returns [(SceneBuilder, camera, pt_params, description)]."""
+    g = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for i in range(n):
+        n_tris = int(round(np.exp(g.uniform(np.log(min_tris), np.log(max_tris)))))
+        if max_tris_cap:
+            n_tris = min(n_tris, max_tris_cap)
+        res = int(round(np.exp(g.uniform(np.log(min_res), np.log(max_res)))))
+        kind = int(g.integers(0, 4))
+        sb = SceneBuilder(background=(0.0, 0.0, 0.0))
+        _box_into(sb, 1.0)
+        if kind == 0:
+            kd = tuple(float(x) for x in g.uniform(0.2, 0.9, 3))
+            m = sb.material(sb.layered_bsdf(sb.lambertian(kd=kd)))
+            desc = "lambertian"
+        elif kind == 1:
+            a = float(g.uniform(0.05, 0.6))
+            m = sb.material(sb.layered_bsdf(sb.cook_torrance(roughness=a, reflectance_at_normal_incidence=CONDUCTOR_F0)))
+            desc = "conductor a=%.2f" % a
+        elif kind == 2:
+            ior = float(g.uniform(1.3, 1.8))
+            m = sb.material(sb.layered_bsdf(sb.smooth_dielectric(ior=ior)))
+            desc = "dielectric ior=%.2f" % ior
+        else:
+            a = float(g.uniform(0.05, 0.6))
+            m = sb.material(sb.layered_bsdf(sb.smooth_dielectric(ior=1.5),
+                                            sb.cook_torrance(roughness=a, reflectance_at_normal_incidence=CONDUCTOR_F0)))
+            desc = "layered a=%.2f" % a
+        sb.triangles(uv_sphere(n_tris, radius=0.3, center=(0.5, 0.32, 0.5), seed=seed + i), m)
+        params = pt_params(spp=spp, sampler="jittered", termination="max-length", path_length=5, seed=seed * 131 + i)
+        out.append((sb, box_camera(res, res), params, "%d tris, %dx%d, %s" % (sb.arrays()[0].shape[0], res, res, desc)))
+    return out
