@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_train(Model M, TrainIO io) {
     if (lane == 0) atomicAdd(io.loss_sum, loss_acc);
 }
 
-constexpr int kChunk = 2048;  // samples per k_wgrad block
+constexpr int kChunk = 256;   // samples per k_wgrad block (256 blocks for 2^16 samples)
 
 // partial[chunk][out][in] = sum over the chunk of dZ^T[out][s] X^T[in][s] (one layer per launch)
 template <int IN, int OUT>

@@ -207,7 +207,9 @@ __global__ void __launch_bounds__(128) k_extend_df(Wave W, Counters* __restrict_
     const uint32_t lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     WideTraversal tr;
-    const DevScene* S = nullptr;
+    // the lane's scene, held by value: the fields the traversal reads stay in registers instead of
+    // being reloaded from the job table at every node
+    DevScene S{};
     bool active = false, exhausted = false;
     unsigned long long mine = 0, pool = 0, pool_end = 0;
     for (;;) {
@@ -225,9 +227,9 @@ __global__ void __launch_bounds__(128) k_extend_df(Wave W, Counters* __restrict_
                 if (mine >= n) {
                     exhausted = true;
                 } else {
-                    S = &W.jobs[__float_as_uint(cur.b[mine].w) >> 16].S;
-                    active = tr.start(*S, f3v(cur.o[mine]), f3v(cur.d[mine]));
-                    if (!active) hits[mine] = hit_record(*S, tr.h);
+                    S = W.jobs[__float_as_uint(cur.b[mine].w) >> 16].S;
+                    active = tr.start(S, f3v(cur.o[mine]), f3v(cur.d[mine]));
+                    if (!active) hits[mine] = hit_record(S, tr.h);
                 }
             }
             if (have < cnt) {
@@ -238,9 +240,9 @@ __global__ void __launch_bounds__(128) k_extend_df(Wave W, Counters* __restrict_
             }
         }
         if (__all_sync(0xFFFFFFFFu, !active && exhausted)) break;
-        if (active && !tr.step(*S, status)) {
-            if (tr.finish(*S)) {
-                hits[mine] = hit_record(*S, tr.h);
+        if (active && !tr.step(S, status)) {
+            if (tr.finish(S)) {
+                hits[mine] = hit_record(S, tr.h);
                 active = false;
             }
         }
@@ -498,9 +500,12 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
     *gpu_ms = 0.0f;
     if (total == 0) return check_status(ctx);
     const uint64_t cap = std::min<uint64_t>(total, std::max<uint32_t>(tune.capacity, 1024u));
+    // Buffer stride: the pool size, or for guided renders (a series of growing passes) the full
+    // tuned capacity, so later passes reuse the first pass's scratch instead of growing it.
+    const uint64_t stride = guide ? std::max<uint64_t>(cap, std::max<uint32_t>(tune.capacity, 1024u)) : cap;
     spt_status st;
     void* mem;
-    const size_t buf_bytes = cap * sizeof(float4);
+    const size_t buf_bytes = stride * sizeof(float4);
     const size_t job_bytes = jobs.size() * sizeof(PtJob);
     if ((st = scratch(ctx, 5, buf_bytes * 9 + sizeof(Counters) + job_bytes + 512, &mem)) != SPT_OK) return st;
     char* base = static_cast<char*>(mem);
@@ -523,17 +528,18 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
             return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "guide batch must be at most 2^22 records");
         rec_cap = kRecBatches * batch;
         void* gm;
-        const size_t gbytes = 2 * cap * sizeof(uint4) + cap * (3 * sizeof(float4) + 40 * sizeof(float) + sizeof(uint32_t)) +
+        const size_t gbytes = 2 * stride * sizeof(uint4) +
+                              stride * (3 * sizeof(float4) + 40 * sizeof(float) + sizeof(uint32_t)) +
                               static_cast<size_t>(rec_cap) * 6 * sizeof(float4) + 1024;
         if ((st = scratch(ctx, 2, gbytes, &gm)) != SPT_OK) return st;
         char* g = static_cast<char*>(gm);
         A.r = reinterpret_cast<uint4*>(g);
-        B.r = A.r + cap;
-        G.infer_in = reinterpret_cast<float4*>(B.r + cap);
-        G.lobes = reinterpret_cast<float*>(G.infer_in + 3 * cap);
-        G.slot_list = reinterpret_cast<uint32_t*>(G.lobes + 40 * cap);
-        G.rec = reinterpret_cast<float4*>(reinterpret_cast<char*>(G.slot_list + cap) + 256 -
-                                          (reinterpret_cast<uintptr_t>(G.slot_list + cap) & 255));
+        B.r = A.r + stride;
+        G.infer_in = reinterpret_cast<float4*>(B.r + stride);
+        G.lobes = reinterpret_cast<float*>(G.infer_in + 3 * stride);
+        G.slot_list = reinterpret_cast<uint32_t*>(G.lobes + 40 * stride);
+        G.rec = reinterpret_cast<float4*>(reinterpret_cast<char*>(G.slot_list + stride) + 256 -
+                                          (reinterpret_cast<uintptr_t>(G.slot_list + stride) & 255));
         G.recx = G.rec + 4ull * rec_cap;
         G.mix = guide->cfg.mix;
         G.rec_cap = rec_cap;

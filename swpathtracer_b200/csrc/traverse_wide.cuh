@@ -28,19 +28,7 @@ struct WideRay {
     V3 o;
     float ix, iy, iz;   // 1/d with zero components replaced by a tiny signed value
     uint32_t inv_oct;   // slot order key: slot ^ inv_oct, ascending = near to far
-    const uint4* top;   // the first n_top nodes staged in shared memory by the block, or null
-    uint32_t n_top;
 };
-
-// Nodes staged in shared memory: the top levels of the breadth-first node order, which every ray
-// from the root visits.
-constexpr uint32_t kTopNodes = 96;
-
-__device__ __forceinline__ void stage_top_nodes(const DevScene& S, uint4* smem, uint32_t& n_top) {
-    n_top = S.n_wnodes < kTopNodes ? S.n_wnodes : kTopNodes;
-    for (uint32_t i = threadIdx.x; i < 5 * n_top; i += blockDim.x) smem[i] = __ldg(S.wnode + i);
-    __syncthreads();
-}
 
 __device__ __forceinline__ float safe_inv(float d) {
     return 1.0f / (fabsf(d) > 1e-20f ? d : copysignf(1e-20f, d));
@@ -49,14 +37,8 @@ __device__ __forceinline__ float safe_inv(float d) {
 __device__ __forceinline__ void wide_node_hits(const DevScene& S, const WideRay& r, uint32_t idx, float best_t,
                                                uint32_t& g_base, uint32_t& g_hits, uint32_t& g_imask,
                                                uint32_t& t_base, uint32_t& t_mask) {
-    uint4 w0, w1, w2, w3, w4;
-    if (idx < r.n_top) {
-        const uint4* n = r.top + 5 * idx;
-        w0 = n[0]; w1 = n[1]; w2 = n[2]; w3 = n[3]; w4 = n[4];
-    } else {
-        const uint4* n = S.wnode + 5 * idx;
-        w0 = __ldg(n); w1 = __ldg(n + 1); w2 = __ldg(n + 2); w3 = __ldg(n + 3); w4 = __ldg(n + 4);
-    }
+    const uint4* n = S.wnode + 5 * idx;
+    const uint4 w0 = __ldg(n), w1 = __ldg(n + 1), w2 = __ldg(n + 2), w3 = __ldg(n + 3), w4 = __ldg(n + 4);
     const int ex = static_cast<int8_t>(w0.w & 0xFFu), ey = static_cast<int8_t>((w0.w >> 8) & 0xFFu),
               ez = static_cast<int8_t>((w0.w >> 16) & 0xFFu);
     const uint32_t imask = w0.w >> 24;
@@ -148,8 +130,6 @@ __device__ __forceinline__ Hit1 closest_hit_wide_pass(const DevScene& S, V3 o, V
     r.iy = safe_inv(d.y);
     r.iz = safe_inv(d.z);
     r.inv_oct = (r.ix >= 0.0f ? 0u : 1u) | (r.iy >= 0.0f ? 0u : 2u) | (r.iz >= 0.0f ? 0u : 4u);
-    r.top = nullptr;
-    r.n_top = 0;
     uint2 stack[kWideStack];
     int sp = 0;
     uint32_t g_base, g_hits, g_imask, t_base, t_mask;
@@ -200,8 +180,6 @@ struct WideTraversal {
     int sp;
     uint32_t g_base, g_hits, g_imask, t_base, t_mask;
     bool exact;
-    const uint4* top = nullptr;   // shared-memory copy of the top nodes (set by the kernel)
-    uint32_t n_top = 0;
 
     // Returns false when the ray is already finished (empty scene or root box missed).
     __device__ __forceinline__ bool start(const DevScene& S, V3 o_, V3 d_, bool exact_ = false) {
@@ -224,8 +202,6 @@ struct WideTraversal {
         r.iy = safe_inv(d.y);
         r.iz = safe_inv(d.z);
         r.inv_oct = (r.ix >= 0.0f ? 0u : 1u) | (r.iy >= 0.0f ? 0u : 2u) | (r.iz >= 0.0f ? 0u : 4u);
-        r.top = top;
-        r.n_top = n_top;
         wide_node_hits(S, r, 0, h.t, g_base, g_hits, g_imask, t_base, t_mask);
         return true;
     }
@@ -281,10 +257,7 @@ __device__ __forceinline__ void persistent_trace(const DevScene& S, uint64_t n, 
                                                  uint32_t* overflow, Load load, Store store) {
     const uint32_t lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    __shared__ uint4 top[5 * kTopNodes];
     WideTraversal tr;
-    stage_top_nodes(S, top, tr.n_top);
-    tr.top = top;
     bool active = false, exhausted = false;
     uint64_t mine = 0;
     unsigned long long pool = 0, pool_end = 0;  // warp-uniform

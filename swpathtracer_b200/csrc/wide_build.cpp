@@ -224,8 +224,8 @@ void build_wide(const std::vector<spt_bvh2_node>& nodes, WideBvh& out) {
     } else {
         c.fill(0, c.collapse(0));
     }
-    // breadth-first order: the top levels come first (staged in shared memory by the kernels) and a
-    // node's inner children stay consecutive
+    // breadth-first order: the top levels, which every ray visits, share cache lines, and a node's
+    // inner children stay consecutive
     std::vector<uint32_t> order;
     order.reserve(built.size());
     order.push_back(0);
