@@ -4,12 +4,36 @@ Device            spt_context on one CUDA device
 Bvh               spt_bvh, the host-built reference SAH tree (SBVH::build / getStatistics)
 GpuScene          spt_scene: a scene resident in HBM, answering ray queries and rendering
 """
+import atexit
 import ctypes as C
 import weakref
 
 import numpy as np
 
 from . import abi, native
+
+
+class _Owned:
+    """A handle that lives on a context, with the call that frees it; released at most once."""
+    __slots__ = ("h", "free")
+
+    def __init__(self, h, free):
+        self.h, self.free = h, free
+
+    def release(self):
+        h, self.h = self.h, None
+        if h:
+            self.free(h)
+
+
+_live_devices = weakref.WeakSet()
+
+
+@atexit.register
+def _close_live_devices():
+    # before interpreter teardown, while the CUDA runtime is intact: free every handle, then contexts
+    for d in list(_live_devices):
+        d.close()
 
 
 class Device:
@@ -21,16 +45,21 @@ class Device:
         native.check(self.lib.spt_create(device, C.byref(h)), None, "spt_create(%d)" % device)
         self.h = h
         self.device = device
-        self._children = weakref.WeakSet()   # scenes and guides that live on this context
+        self._owned = []    # handles of scenes and guides on this context, freed before it
+        _live_devices.add(self)
 
-    def adopt(self, obj):
-        """Registers an object whose handle must be released before the context."""
-        self._children.add(obj)
+    def adopt(self, h, free):
+        """Registers a handle that must be released before the context; returns its _Owned."""
+        self._owned = [o for o in self._owned if o.h]
+        o = _Owned(h, free)
+        self._owned.append(o)
+        return o
 
     def close(self):
         if getattr(self, "h", None):
-            for c in list(self._children):
-                c.close()
+            for o in reversed(self._owned):
+                o.release()
+            self._owned = []
             self.lib.spt_destroy(self.h)
             self.h = None
 
@@ -88,12 +117,13 @@ class GpuScene:
         device.check(self.lib.spt_scene_create(device.h, packed.ref(), bvh.h if bvh else None, C.byref(h)),
                      "spt_scene_create")
         self.h = h
-        device.adopt(self)
+        self._own = device.adopt(h, self.lib.spt_scene_destroy)
 
     def close(self):
-        if getattr(self, "h", None):
-            self.lib.spt_scene_destroy(self.h)
-            self.h = None
+        own = getattr(self, "_own", None)
+        if own is not None:
+            own.release()
+        self.h = None
 
     def __del__(self):
         try:
@@ -218,12 +248,13 @@ class Guide:
         device.check(self.lib.spt_guide_create(device.h, C.byref(config or guide_config()), C.byref(h)),
                      "spt_guide_create")
         self.h = h
-        device.adopt(self)
+        self._own = device.adopt(h, self.lib.spt_guide_destroy)
 
     def close(self):
-        if getattr(self, "h", None):
-            self.lib.spt_guide_destroy(self.h)
-            self.h = None
+        own = getattr(self, "_own", None)
+        if own is not None:
+            own.release()
+        self.h = None
 
     def __del__(self):
         try:

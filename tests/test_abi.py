@@ -82,3 +82,23 @@ def test_ppm_writer_format(tmp_path):
     write_ppm(str(p), rgb, srgb=False)
     vals = [int(v) for v in p.read_text().split()[4:]]
     assert vals == [0, 128, 255, 255, 0, 64]
+
+
+def test_handles_are_freed_once_and_before_their_context():
+    """Scenes and guides release their handles before the context, whichever is closed first."""
+    from swpathtracer_b200 import api
+    calls = []
+
+    class FakeLib:
+        def spt_destroy(self, h):
+            calls.append(("ctx", h))
+
+    d = object.__new__(api.Device)
+    d.lib, d.h, d.device, d._owned = FakeLib(), 1, 0, []
+    a = d.adopt(10, lambda h: calls.append(("scene", h)))
+    b = d.adopt(20, lambda h: calls.append(("guide", h)))
+    a.release()                      # the scene closed by its owner first
+    d.close()                        # then the context: the guide goes before it
+    b.release()                      # a late close of the guide is a no-op
+    d.close()
+    assert calls == [("scene", 10), ("guide", 20), ("ctx", 1)]
