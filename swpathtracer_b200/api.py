@@ -149,6 +149,20 @@ class GpuScene:
                                               None if nh is None else nh.ctypes.data), "spt_intersect")
         return dict(hits=hits, tests=tests, nhits=nh)
 
+    def intersect_noalloc(self, rays, counts=False):
+        """intersect() through spt_intersect_noalloc (include/spt_noalloc.h): no device allocation in
+        the call, at most 65536 rays, calls on one device must not overlap."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        hits = np.zeros(n, abi.HIT_DTYPE)
+        tests = np.zeros(n, np.uint32) if counts else None
+        nh = np.zeros(n, np.uint32) if counts else None
+        self.dev.check(self.lib.spt_intersect_noalloc(self.dev.h, self.h, rays.ctypes.data, n, hits.ctypes.data,
+                                                      None if tests is None else tests.ctypes.data,
+                                                      None if nh is None else nh.ctypes.data),
+                       "spt_intersect_noalloc")
+        return dict(hits=hits, tests=tests, nhits=nh)
+
     def intersect_device(self, d_rays, n, d_hits, stream=0):
         self.dev.check(self.lib.spt_intersect_device(self.dev.h, self.h, d_rays, n, d_hits, stream),
                        "spt_intersect_device")

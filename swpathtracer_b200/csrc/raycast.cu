@@ -182,6 +182,20 @@ spt_status launch_intersect(spt_context* ctx, const spt_scene* sc, const float* 
     return SPT_OK;
 }
 
+// launch_intersect with the persistent kernel's ray counter supplied by the caller (zeroed on stream s
+// before this launch) instead of taken from the context's ring, which is allocated on first use.
+spt_status launch_intersect_fixed(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n,
+                                  spt_hit* d_hits, unsigned long long* next, cudaStream_t s) {
+    if (n == 0) return SPT_OK;
+    if (sc->dev.traversal != 2) return launch_intersect(ctx, sc, d_rays, n, d_hits, s);  // no counter needed
+    static int grid = 0;
+    if (!grid) grid = persistent_grid(ctx, reinterpret_cast<const void*>(k_intersect_df), kBlock);
+    k_intersect_df<<<grid, kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n, d_hits, ctx->d_status,
+                                          next);
+    SPT_CUDA(ctx, cudaGetLastError());
+    return SPT_OK;
+}
+
 spt_status launch_count(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_ref_hits,
                         uint32_t* d_tests, uint32_t* d_hits, uint32_t* d_prim_tests, cudaStream_t s) {
     if (n == 0) return SPT_OK;

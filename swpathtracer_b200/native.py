@@ -28,6 +28,7 @@ PROTOTYPES = {
     "spt_intersect": (i32, [vp, vp, vp, u64, vp, vp, vp]),
     "spt_intersect_device": (i32, [vp, vp, vp, u64, vp, vp]),
     "spt_count_device": (i32, [vp, vp, vp, u64, vp, vp, vp, vp, vp]),
+    "spt_intersect_noalloc": (i32, [vp, vp, vp, u64, vp, vp, vp]),
     "spt_raycast_image": (i32, [vp, vp, vp, i32, vp, vp]),
     "spt_raycast_image_device": (i32, [vp, vp, vp, i32, vp, vp]),
     "spt_pathtrace": (i32, [vp, vp, vp, vp, vp, vp]),
