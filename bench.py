@@ -122,6 +122,70 @@ def cpu_baseline(packed, rays_np, budget_rays):
             "sample": "%d of the step's incoherent rays, SBVH::intersect per ray, OpenMP over rays" % len(sample)}
 
 
+def guided_vs_plain(spt, scenes, dev, torch, spp=4096):
+    """Equal-time relMSE of guided vs plain path tracing on the small-light box (128^2, max length 5;
+    the light is a 0.06 x 0.06 quad, found only by sampling its direction).  Both render `spp`
+    samples; each image's relMSE mean((I - R)^2 / (R^2 + 1e-2)) against a 16,384-spp plain render
+    is multiplied by its wall time (relMSE falls as 1/time), and the ratio plain / guided of those
+    products is the relMSE ratio at equal time (> 1: guiding wins).  The guided time includes its
+    online training (256 Adam steps of 2^16 records)."""
+    import numpy as np
+    gs = spt.GpuScene(dev, scenes.small_light_box_scene().build())
+    cam = scenes.box_camera(128, 128)
+    img = torch.empty(128 * 128 * 3, dtype=torch.float32, device="cuda")
+
+    def render(n, seed, guide=None):
+        p = scenes.pt_params(spp=n, sampler="jittered", termination="max-length", path_length=5, seed=seed)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if guide is None:
+            gs.pathtrace_device(cam, p, img.data_ptr())
+        else:
+            gs.pathtrace_guided_device(cam, p, guide, img.data_ptr())
+        torch.cuda.synchronize()
+        return img.cpu().numpy().reshape(128, 128, 3).copy(), time.perf_counter() - t0
+
+    def relmse(a, b):
+        return float(np.mean((a - b) ** 2 / (b ** 2 + 1e-2)))
+
+    render(64, 1)
+    ref, _ = render(16384, 99)
+    plain, t_plain = render(spp, 7)
+    g = spt.Guide(dev, spt.guide_config(batch=1 << 16, max_steps=256, mix=0.5, seed=1))
+    guided, t_guided = render(spp, 7, g)
+    e_plain, e_guided = relmse(plain, ref), relmse(guided, ref)
+    g.close()
+    gs.close()
+    return {"guided_small_light_128x128_spp": spp,
+            "guided_relmse_plain": round(e_plain, 5), "guided_relmse_guided": round(e_guided, 5),
+            "guided_wall_ms_plain": round(1e3 * t_plain, 2), "guided_wall_ms_guided": round(1e3 * t_guided, 2),
+            "guided_equal_time_relmse_ratio_plain_over_guided": round((e_plain * t_plain) / (e_guided * t_guided), 4)}
+
+
+def cpu_pathtrace_baseline(subdiv):
+    """The reference's own PathTracer::render (oracle/_ref) on this host's cores, on bounded samples of
+    the two path-tracing workloads (4 spp of the box scene, 1 spp of the layered 1.3M-tri scene).
+    The reference has no depth cap next to russian roulette: its layered run caps at 1000 bounces."""
+    from swpathtracer_b200 import scenes
+    try:
+        from oracle.bindings import RefHarness
+        h = RefHarness()
+    except FileNotFoundError:
+        return None
+    cores = os.cpu_count() or 1
+    out = {"cores": cores, "kind": "reference", "unit": "Mpaths/s"}
+    for key, sb, cam, prm in (
+            ("pt_box_256x256", scenes.box_scene(5), scenes.box_camera(256, 256),
+             scenes.pt_params(spp=4, sampler="jittered", termination="max-length", path_length=5, seed=3)),
+            ("pt_layered_800x600_rr3", scenes.layered_box_scene(subdiv), scenes.layered_box_camera(800, 600),
+             scenes.pt_params(spp=1, sampler="jittered", termination="russian-roulette", path_length=3, seed=4))):
+        rs = h.scene(sb.build(), n_threads=cores)
+        _, secs = rs.pathtrace(cam, prm, n_threads=cores)
+        out[key + "_Mpaths_s"] = round(cam.width * cam.height * prm.spp / secs / 1e6, 4)
+    out["sample"] = "PathTracer::render, box 256x256 at 4 spp, layered 800x600 at 1 spp, OpenMP over rows"
+    return out
+
+
 def run_reference(a):
     """--impl reference: the reference's CPU path on the same workload (rank 0 only)."""
     rank = int(os.environ.get("RANK", "0"))
@@ -247,7 +311,7 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            tr = json.load(f).get("k_intersect")
+            tr = json.load(f).get("k_intersect_df")
         if tr:
             traffic = tr["bytes_per_ray"] * n
 
@@ -314,9 +378,14 @@ def main():
         extras["batch64_paths"] = paths
         for g_, _, _ in jobs:
             g_.close()
+        extras.update(guided_vs_plain(spt, scenes, dev, torch))
         out["submetrics"] = extras
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(packed, rays_np, 1 << 22)
+        if not a.no_extras:
+            pt = cpu_pathtrace_baseline(a.subdiv)
+            if pt:
+                out["cpu_baseline"]["pathtrace"] = pt
     if rank == 0:
         print(json.dumps(out), flush=True)
     gs.close()

@@ -77,6 +77,7 @@ struct GuideIO {
 
 constexpr uint32_t kNoRec = 0xFFFFFFFFu;
 constexpr uint32_t kRecBatches = 4;   // training records held per render: this many optimiser batches
+constexpr uint32_t kTrainEpochs = 4;  // optimiser passes over each filled record buffer
 
 __device__ __forceinline__ uint32_t n_new_paths(const Wave& W, const Counters& c) {
     const unsigned long long rem = W.total - c.next_path;
@@ -595,17 +596,18 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
     bool done = false;
     bool training = guide && train_budget > 0, pending = false;
     uint32_t steps = 0;
-    // Optimiser steps on the n records in the buffer, batch records per step (the last step takes
-    // the remainder), then a fresh generation of records.
+    // kTrainEpochs passes of optimiser steps over the n records in the buffer, batch records per step
+    // (a short tail joins no step of its own), then a fresh generation of records.
     auto train = [&](uint32_t n) -> spt_status {
         k_record_weights<<<256, 256, 0, ctx->stream>>>(G.rec, G.recx, n);
-        for (uint32_t off = 0; off < n && steps < train_budget; off += batch) {
-            const uint32_t m = std::min(batch, n - off);
-            if (m < batch / 4 && off > 0) break;   // too few records left for a step of its own
-            spt_status s2 = guide->step(G.rec + 4ull * off, m, nullptr);
-            if (s2 != SPT_OK) return s2;
-            ++steps;
-        }
+        for (uint32_t e = 0; e < kTrainEpochs; ++e)
+            for (uint32_t off = 0; off < n && steps < train_budget; off += batch) {
+                const uint32_t m = std::min(batch, n - off);
+                if (m < batch / 4 && off > 0) break;
+                spt_status s2 = guide->step(G.rec + 4ull * off, m, nullptr);
+                if (s2 != SPT_OK) return s2;
+                ++steps;
+            }
         training = steps < train_budget;
         k_next_generation<<<1, 1, 0, ctx->stream>>>(d_ctr, training ? 1u : 0u);
         return SPT_OK;
