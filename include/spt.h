@@ -314,6 +314,23 @@ spt_status spt_guided_pathtrace_device(spt_context* ctx, const spt_scene* scene,
                                        spt_render_stats* stats);
 
 /* ---- image post-processing (reference core/image_buffer.cpp and the ray casters' saveImageToFile) */
+/* DepthRayCaster::saveImageToFile (integrators/depth_raycaster.cpp:9-34) on the device: d_depth float[h][w]
+ * (-1 = background) -> d_rgb float[h][w][3] grey ramp; min_depth / max_depth = -1 take the image's own
+ * (min over hits, max over all pixels). */
+spt_status spt_depth_to_rgb_device(spt_context* ctx, const float* d_depth, uint32_t width, uint32_t height,
+                                   float min_depth, float max_depth, float* d_rgb, void* stream);
+/* IntTestCountRayCaster::saveImageToFile (int_test_count_raycaster.cpp:20-73): d_count int64[h][w] ->
+ * HSL heat map; min_count / max_count = -1 take the image's own per-pixel min / max. */
+spt_status spt_count_to_rgb_device(spt_context* ctx, const int64_t* d_count, uint32_t width, uint32_t height,
+                                   int64_t min_count, int64_t max_count, float* d_rgb, void* stream);
+/* NormalRayCaster::saveImageToFile (integrators/normal_raycaster.cpp:6-17), in place on a normal image:
+ * n * 0.5 + 0.5 for every pixel that is not background (0, 0, 0). */
+spt_status spt_normal_to_rgb_device(spt_context* ctx, float* d_rgb, uint32_t width, uint32_t height, void* stream);
+/* ImageBuffer::convertTosRGB (when to_srgb) + the clamp / int(c * 255 + 0.5) of saveToFile, per value. */
+spt_status spt_rgb_to_bytes_device(spt_context* ctx, const float* d_rgb, uint64_t n_values, int32_t to_srgb,
+                                   uint8_t* d_bytes, void* stream);
+/* The ASCII P3 file of saveToFile from already quantized bytes (host memory). */
+spt_status spt_write_ppm_bytes(const char* path, const uint8_t* rgb8, uint32_t width, uint32_t height);
 /* sRGB (pow 1/2.2 of the clamped value) + ASCII P3 PPM writer, core/image_buffer.cpp:22-47. */
 spt_status spt_write_ppm(const char* path, const float* rgb, uint32_t width, uint32_t height, int32_t to_srgb);
 

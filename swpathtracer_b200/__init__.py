@@ -5,6 +5,7 @@ package only loads it (native), mirrors its structs (abi), builds scene descript
 synthetic workloads (scenes) and wraps the handles (api).
 """
 from . import abi, scenes  # noqa: F401
-from .api import (Bvh, Device, GpuScene, Guide, autotune, default_tune, guide_config, render_batch,  # noqa: F401
-                  write_ppm)
+from .api import (Bvh, Device, GpuScene, Guide, autotune, count_to_rgb_device, default_tune,  # noqa: F401
+                  depth_to_rgb_device, guide_config, normal_to_rgb_device, render_batch, rgb_to_bytes_device,
+                  write_ppm, write_ppm_bytes)
 from .native import SptError  # noqa: F401

@@ -320,6 +320,37 @@ class Guide:
         return loss.value
 
 
+def depth_to_rgb_device(device, d_depth, width, height, d_rgb, min_depth=-1.0, max_depth=-1.0, stream=0):
+    """DepthRayCaster::saveImageToFile's grey ramp on the device (float[h][w] -> float[h][w][3])."""
+    device.check(device.lib.spt_depth_to_rgb_device(device.h, d_depth, width, height, min_depth, max_depth, d_rgb,
+                                                    stream), "spt_depth_to_rgb_device")
+
+
+def count_to_rgb_device(device, d_count, width, height, d_rgb, min_count=-1, max_count=-1, stream=0):
+    """IntTestCountRayCaster::saveImageToFile's heat map on the device (int64[h][w] -> float[h][w][3])."""
+    device.check(device.lib.spt_count_to_rgb_device(device.h, d_count, width, height, min_count, max_count, d_rgb,
+                                                    stream), "spt_count_to_rgb_device")
+
+
+def normal_to_rgb_device(device, d_rgb, width, height, stream=0):
+    """NormalRayCaster::saveImageToFile's n * 0.5 + 0.5 encoding, in place on the device."""
+    device.check(device.lib.spt_normal_to_rgb_device(device.h, d_rgb, width, height, stream),
+                 "spt_normal_to_rgb_device")
+
+
+def rgb_to_bytes_device(device, d_rgb, n_values, d_bytes, srgb=True, stream=0):
+    """convertTosRGB (when srgb) and the 8-bit quantization of ImageBuffer::saveToFile on the device."""
+    device.check(device.lib.spt_rgb_to_bytes_device(device.h, d_rgb, n_values, 1 if srgb else 0, d_bytes, stream),
+                 "spt_rgb_to_bytes_device")
+
+
+def write_ppm_bytes(path, rgb8):
+    """The P3 file of ImageBuffer::saveToFile from quantized bytes (uint8 [h, w, 3], host)."""
+    rgb8 = np.ascontiguousarray(rgb8, np.uint8)
+    h, w = rgb8.shape[:2]
+    native.check(native.lib().spt_write_ppm_bytes(path.encode(), rgb8.ctypes.data, w, h), None, "spt_write_ppm_bytes")
+
+
 def write_ppm(path, rgb, srgb=True):
     """ImageBuffer::saveToFile (core/image_buffer.cpp:32-47), with convertTosRGB first when srgb."""
     rgb = np.ascontiguousarray(rgb, np.float32)

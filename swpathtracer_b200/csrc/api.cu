@@ -211,7 +211,7 @@ spt_status spt_destroy(spt_context* ctx) {
     if (!ctx) return SPT_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < spt_context::kScratchSlots; ++i)
         if (ctx->scratch[i]) cudaFree(ctx->scratch[i]);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->d_status) cudaFree(ctx->d_status);

@@ -22,8 +22,9 @@ struct spt_context {
     uint32_t* d_status = nullptr;  // device error word: bit 0 stack overflow, bit 1 queue overflow, bit 2 timeout
     std::string err;
     // scratch buffers reused across calls (grown on demand)
-    void* scratch[8] = {};
-    size_t scratch_bytes[8] = {};
+    static constexpr int kScratchSlots = 12;
+    void* scratch[kScratchSlots] = {};
+    size_t scratch_bytes[kScratchSlots] = {};
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
     // ray counters of the persistent (dynamic-fetch) kernels: a ring, one slot per launch

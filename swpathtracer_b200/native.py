@@ -34,6 +34,11 @@ PROTOTYPES = {
     "spt_pathtrace": (i32, [vp, vp, vp, vp, vp, vp]),
     "spt_pathtrace_device": (i32, [vp, vp, vp, vp, vp, vp]),
     "spt_write_ppm": (i32, [C.c_char_p, vp, u32, u32, i32]),
+    "spt_depth_to_rgb_device": (i32, [vp, vp, u32, u32, C.c_float, C.c_float, vp, vp]),
+    "spt_count_to_rgb_device": (i32, [vp, vp, u32, u32, C.c_int64, C.c_int64, vp, vp]),
+    "spt_normal_to_rgb_device": (i32, [vp, vp, u32, u32, vp]),
+    "spt_rgb_to_bytes_device": (i32, [vp, vp, u64, i32, vp, vp]),
+    "spt_write_ppm_bytes": (i32, [C.c_char_p, vp, u32, u32]),
     "spt_tune_default": (i32, [vp]),
     "spt_batch_pathtrace": (i32, [vp, vp, u32, vp, vp, vp]),
     "spt_autotune": (i32, [vp, vp, u32, C.c_char_p, vp]),
