@@ -135,15 +135,21 @@ class GpuScene:
         return self.lib.spt_scene_device_bytes(self.h)
 
     # ---- ray queries -------------------------------------------------------------------------
-    def intersect(self, rays, counts=False, out=None):
+    def intersect(self, rays, counts=False, out=None, out_counts=None):
         """Closest hit per ray (rays: float32 [n, 8]); counts adds the reference's per-ray test counts.
-        out: optional preallocated (e.g. pinned) array of abi.HIT_DTYPE for the hits."""
+        out: optional preallocated (e.g. pinned) array of abi.HIT_DTYPE for the hits; out_counts:
+        optional (tests, nhits) uint32 arrays for the counts.  With every buffer page-locked, large
+        batches run as a pipeline of chunks whose copies overlap the queries."""
         rays = np.ascontiguousarray(rays, np.float32)
         n = rays.shape[0]
         hits = out if out is not None else np.zeros(n, abi.HIT_DTYPE)
         assert hits.dtype == abi.HIT_DTYPE and hits.shape == (n,) and hits.flags["C_CONTIGUOUS"]
-        tests = np.zeros(n, np.uint32) if counts else None
-        nh = np.zeros(n, np.uint32) if counts else None
+        if out_counts is not None:
+            tests, nh = out_counts
+            assert tests.dtype == np.uint32 and nh.dtype == np.uint32 and tests.shape == (n,) and nh.shape == (n,)
+        else:
+            tests = np.zeros(n, np.uint32) if counts else None
+            nh = np.zeros(n, np.uint32) if counts else None
         self.dev.check(self.lib.spt_intersect(self.dev.h, self.h, rays.ctypes.data, n, hits.ctypes.data,
                                               None if tests is None else tests.ctypes.data,
                                               None if nh is None else nh.ctypes.data), "spt_intersect")

@@ -200,6 +200,10 @@ spt_status spt_create(int device, spt_context** out) {
     if (e != cudaSuccess || device < 0 || device >= n) return SPT_ERR_CUDA;
     if (cudaSetDevice(device) != cudaSuccess) return SPT_ERR_CUDA;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return SPT_ERR_CUDA;
+    for (int i = 0; i < spt_context::kPipe; ++i) {
+        if (cudaStreamCreateWithFlags(&ctx->pipe[i], cudaStreamNonBlocking) != cudaSuccess) return SPT_ERR_CUDA;
+        if (cudaEventCreateWithFlags(&ctx->ev_pipe[i], cudaEventDisableTiming) != cudaSuccess) return SPT_ERR_CUDA;
+    }
     if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) return SPT_ERR_CUDA;
     if (cudaMalloc(&ctx->d_status, sizeof(uint32_t)) != cudaSuccess) return SPT_ERR_OUT_OF_MEMORY;
     if (cudaMemset(ctx->d_status, 0, sizeof(uint32_t)) != cudaSuccess) return SPT_ERR_CUDA;
@@ -218,6 +222,13 @@ spt_status spt_destroy(spt_context* ctx) {
     if (ctx->d_fetch) cudaFree(ctx->d_fetch);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    for (int i = 0; i < spt_context::kPipe; ++i) {
+        if (ctx->pipe[i]) {
+            cudaStreamSynchronize(ctx->pipe[i]);
+            cudaStreamDestroy(ctx->pipe[i]);
+        }
+        if (ctx->ev_pipe[i]) cudaEventDestroy(ctx->ev_pipe[i]);
+    }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SPT_OK;

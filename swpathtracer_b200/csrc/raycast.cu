@@ -225,6 +225,66 @@ static spt_status launch_raycast(spt_context* ctx, const spt_scene* sc, const De
 
 }  // namespace spt
 
+namespace spt {
+namespace {
+
+constexpr uint64_t kPipeChunk = 1ull << 21;  // rays per pipeline chunk (64 MB in, 32 MB out)
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Host buffers in page-locked memory: the batch goes through in chunks over the context's pipeline
+// streams, chunk c on stream c % kPipe, so the copy in of one chunk, the query of another and the
+// copy out of a third run at the same time (PCIe is full duplex).  Each stream owns one set of
+// device buffers; its chunks are in stream order, so a set is reused only after its last chunk's
+// copy out.
+spt_status intersect_pipelined(spt_context* ctx, const spt_scene* sc, const float* rays, uint64_t n, spt_hit* hits,
+                               uint32_t* tests, uint32_t* nhits) {
+    const int P = spt_context::kPipe;
+    const size_t set_bytes = kPipeChunk * (32 + sizeof(spt_hit) + 4 + 4);
+    void* mem;
+    spt_status st = scratch(ctx, 9, set_bytes * P, &mem);
+    if (st != SPT_OK) return st;
+    // the pipeline streams start after whatever the context's stream has queued
+    SPT_CUDA(ctx, cudaEventRecord(ctx->ev_pipe[0], ctx->stream));
+    for (int i = 0; i < P; ++i) SPT_CUDA(ctx, cudaStreamWaitEvent(ctx->pipe[i], ctx->ev_pipe[0], 0));
+    const uint64_t chunks = (n + kPipeChunk - 1) / kPipeChunk;
+    for (uint64_t c = 0; c < chunks; ++c) {
+        const int i = static_cast<int>(c % P);
+        cudaStream_t s = ctx->pipe[i];
+        char* base = static_cast<char*>(mem) + set_bytes * i;
+        float* d_rays = reinterpret_cast<float*>(base);
+        spt_hit* d_hits = reinterpret_cast<spt_hit*>(base + kPipeChunk * 32);
+        uint32_t* d_tests = reinterpret_cast<uint32_t*>(base + kPipeChunk * (32 + sizeof(spt_hit)));
+        uint32_t* d_nh = d_tests + kPipeChunk;
+        const uint64_t first = c * kPipeChunk, m = std::min(kPipeChunk, n - first);
+        SPT_CUDA(ctx, cudaMemcpyAsync(d_rays, rays + 8 * first, m * 32, cudaMemcpyHostToDevice, s));
+        if ((st = launch_intersect(ctx, sc, d_rays, m, d_hits, s)) != SPT_OK) return st;
+        if (tests || nhits)
+            if ((st = launch_count(ctx, sc, d_rays, m, nullptr, tests ? d_tests : nullptr, nhits ? d_nh : nullptr,
+                                   nullptr, s)) != SPT_OK)
+                return st;
+        SPT_CUDA(ctx, cudaMemcpyAsync(hits + first, d_hits, m * sizeof(spt_hit), cudaMemcpyDeviceToHost, s));
+        if (tests) SPT_CUDA(ctx, cudaMemcpyAsync(tests + first, d_tests, m * 4, cudaMemcpyDeviceToHost, s));
+        if (nhits) SPT_CUDA(ctx, cudaMemcpyAsync(nhits + first, d_nh, m * 4, cudaMemcpyDeviceToHost, s));
+    }
+    // the context's stream continues after every chunk
+    for (int i = 0; i < P; ++i) {
+        SPT_CUDA(ctx, cudaEventRecord(ctx->ev_pipe[i], ctx->pipe[i]));
+        SPT_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_pipe[i], 0));
+    }
+    return check_status(ctx);
+}
+
+}  // namespace
+}  // namespace spt
+
 using namespace spt;
 
 extern "C" {
@@ -234,6 +294,9 @@ spt_status spt_intersect(spt_context* ctx, const spt_scene* sc, const float* ray
     if (!ctx || !sc || (n && (!rays || !hits))) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
     if (n == 0) return SPT_OK;
     SPT_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (n > kPipeChunk && is_pinned(rays) && is_pinned(hits) && (!tests || is_pinned(tests)) &&
+        (!nhits || is_pinned(nhits)))
+        return intersect_pipelined(ctx, sc, rays, n, hits, tests, nhits);
     spt_status st;
     void *d_rays, *d_hits, *d_tests = nullptr, *d_nh = nullptr;
     if ((st = scratch(ctx, 0, n * 32, &d_rays)) != SPT_OK) return st;

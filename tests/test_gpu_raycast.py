@@ -112,3 +112,33 @@ def test_full_size_mesh_closest_equals_exhaustive(device):
     assert (prim[hit] < packed.n_prims).all()
     assert (t[hit] > 0).all() and np.isinf(t[~hit]).all()
     assert 0.1 < hit.mean() < 0.6
+
+
+def test_pipelined_host_queries_match_device_queries(device):
+    """spt_intersect with page-locked host buffers runs in chunks over three streams; the hits and
+    counts equal one device-side query of the whole batch (and the pageable path)."""
+    import torch
+    packed = scenes.displaced_mesh_scene(6).build()
+    gs = spt.GpuScene(device, packed)
+    n = (1 << 21) * 2 + 12345                   # three chunks, the last one partial
+    rays = scenes.incoherent_rays(n, seed=77, half_extent=1.5)
+    h_rays = torch.from_numpy(rays).pin_memory()
+    h_hits = torch.empty((n, 4), dtype=torch.int32).pin_memory().numpy().view(abi.HIT_DTYPE).reshape(n)
+    got = gs.intersect(h_rays.numpy(), out=h_hits)
+    d_rays = torch.from_numpy(rays).cuda()
+    d_hits = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    gs.intersect_device(d_rays.data_ptr(), n, d_hits.data_ptr(), 0)
+    torch.cuda.synchronize()
+    assert got["hits"].tobytes() == d_hits.cpu().numpy().tobytes()
+    # counts through the pipeline against the pageable (single-stream) path on a slice
+    sub = rays[: (1 << 21) + 999]
+    m = sub.shape[0]
+    pinned = torch.from_numpy(np.ascontiguousarray(sub)).pin_memory().numpy()
+    p_hits = torch.empty((m, 4), dtype=torch.int32).pin_memory().numpy().view(abi.HIT_DTYPE).reshape(m)
+    p_tests = torch.empty(m, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    p_nh = torch.empty(m, dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    a = gs.intersect(pinned, out=p_hits, out_counts=(p_tests, p_nh))
+    b = gs.intersect(np.ascontiguousarray(sub), counts=True)
+    assert a["hits"].tobytes() == b["hits"].tobytes()
+    np.testing.assert_array_equal(a["tests"], b["tests"])
+    np.testing.assert_array_equal(a["nhits"], b["nhits"])
