@@ -17,7 +17,8 @@ namespace {
 constexpr int kBlock = 128;
 
 // Persistent variant: wide traversal, lanes refilled from a global ray counter (traverse_wide.cuh).
-__global__ void __launch_bounds__(kBlock) k_intersect_df(DevScene S, const float4* __restrict__ rays, uint64_t n,
+// 10 blocks of 128 per SM (at most 48 registers): 40 resident warps to hide the node-fetch latency
+__global__ void __launch_bounds__(kBlock, 10) k_intersect_df(DevScene S, const float4* __restrict__ rays, uint64_t n,
                                                          spt_hit* __restrict__ hits, uint32_t* status,
                                                          unsigned long long* next) {
     persistent_trace(

@@ -248,9 +248,10 @@ struct WideTraversal {
 // Persistent warps with dynamic ray fetch (after Aila & Laine, "Understanding the Efficiency of Ray
 // Traversal on GPUs", HPG 2009): a lane whose ray is finished takes the next ray at once instead of
 // idling until the warp's longest ray ends.  Ray indices come from a warp-local pool refilled
-// kChunk at a time from one global counter, so the counter sees one atomic per kChunk rays.
+// kChunk at a time from one global counter, so the counter sees one atomic per kChunk rays (64:
+// measured 1.5 % faster than 256 on the incoherent workload, from a shorter tail).
 // load(i, o, d) fetches ray i; store(i, h) writes its result.
-constexpr uint32_t kChunk = 256;
+constexpr uint32_t kChunk = 64;
 
 template <typename Load, typename Store>
 __device__ __forceinline__ void persistent_trace(const DevScene& S, uint64_t n, unsigned long long* next,
