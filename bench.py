@@ -376,7 +376,8 @@ def main():
         extras["batch64_Mpaths_s"] = round(paths / (st[0].gpu_ms / 1e3) / 1e6, 3)
         extras["batch64_Mrays_s"] = round(st[0].segments / (st[0].gpu_ms / 1e3) / 1e6, 2)
         extras["batch64_tune"] = {"capacity": tune.capacity, "shade_block": tune.shade_block,
-                                  "traversal": tune.traversal, "check_every": tune.check_every}
+                                  "traversal": tune.traversal, "check_every": tune.check_every,
+                                  "sort_shading": tune.sort_shading}
         extras["batch64_paths"] = paths
         for g_, _, _ in jobs:
             g_.close()

@@ -245,7 +245,9 @@ typedef struct spt_tune {
     uint32_t shade_block;   /* threads per block of the shade kernel */
     int32_t traversal;      /* -1 scene default, 0 binary pair nodes, 1 8-wide, 2 8-wide + dynamic fetch */
     uint32_t check_every;   /* wavefront iterations between host checks for completion */
-    uint32_t reserved[3];
+    uint32_t sort_shading;  /* shade the paths grouped by material class: 0 when a scene has layered
+                               materials (their walks diverge most), 1 always, 2 never */
+    uint32_t reserved[2];
 } spt_tune;
 
 typedef struct spt_batch_job {

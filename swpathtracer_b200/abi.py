@@ -96,7 +96,8 @@ class BvhStats(C.Structure):
 
 class Tune(C.Structure):
     _fields_ = [("capacity", C.c_uint32), ("extend_block", C.c_uint32), ("shade_block", C.c_uint32),
-                ("traversal", C.c_int32), ("check_every", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("traversal", C.c_int32), ("check_every", C.c_uint32), ("sort_shading", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
 
 class BatchJob(C.Structure):

@@ -448,6 +448,7 @@ spt_status spt_scene_create(spt_context* ctx, const spt_scene_desc* d, const spt
                 layers.push_back(static_cast<int>(d->layered_bsdf_ids[k]));
             o.layer_count = static_cast<int>(layers.size()) - o.layer_begin;
             o.er = m.emission[0]; o.eg = m.emission[1]; o.eb = m.emission[2];
+            sc->any_layered |= o.layer_count > 1;
             any_em |= (m.emission[0] != 0.0f || m.emission[1] != 0.0f || m.emission[2] != 0.0f);
         }
         std::vector<uint32_t> pm(d->prim_material, d->prim_material + n);

@@ -62,7 +62,9 @@ bool cache_lookup(const char* path, const std::string& key, spt_tune& t) {
         std::string k;
         spt_tune c = default_tune();
         double ms;
-        if (is >> k >> c.capacity >> c.extend_block >> c.shade_block >> c.traversal >> c.check_every >> ms && k == key) {
+        if (is >> k >> c.capacity >> c.extend_block >> c.shade_block >> c.traversal >> c.check_every >> c.sort_shading >>
+                ms &&
+            k == key) {
             t = c;
             found = true;  // the last entry for a key wins
         }
@@ -74,7 +76,7 @@ void cache_store(const char* path, const std::string& key, const spt_tune& t, do
     if (!path) return;
     std::ofstream f(path, std::ios::app);
     f << key << " " << t.capacity << " " << t.extend_block << " " << t.shade_block << " " << t.traversal << " "
-      << t.check_every << " " << ms << "\n";
+      << t.check_every << " " << t.sort_shading << " " << ms << "\n";
 }
 
 }  // namespace
@@ -151,8 +153,8 @@ spt_status spt_autotune(spt_context* ctx, const spt_batch_job* jobs, uint32_t n_
     const uint32_t caps[] = {1u << 20, 1u << 21, 1u << 22};
     const uint32_t shades[] = {64, 128, 256};
     const uint32_t checks[] = {4, 8, 16};
-    for (int dim = 0; dim < 4; ++dim) {
-        const int n_opt = 3;
+    for (int dim = 0; dim < 5; ++dim) {
+        const int n_opt = dim == 4 ? 2 : 3;
         spt_tune round_best = best;
         for (int k = 0; k < n_opt; ++k) {
             spt_tune c = best;
@@ -160,6 +162,7 @@ spt_status spt_autotune(spt_context* ctx, const spt_batch_job* jobs, uint32_t n_
             if (dim == 1) c.capacity = caps[k];
             if (dim == 2) c.shade_block = shades[k];
             if (dim == 3) c.check_every = checks[k];
+            if (dim == 4) c.sort_shading = static_cast<uint32_t>(k + 1);   // always / never
             if (std::memcmp(&c, &best, sizeof(c)) == 0) continue;
             double ms = 0.0;
             if ((st = time_of(c, ms)) != SPT_OK) return st;

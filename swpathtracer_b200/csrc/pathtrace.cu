@@ -260,19 +260,81 @@ __device__ __forceinline__ void splat(const PtJob& J, uint32_t pix, V3 L) {
 
 __device__ __forceinline__ bool rec_live(uint32_t r, uint32_t gen) { return r != kNoRec && (r >> 24) == (gen & 0xFFu); }
 
+// ---- shading grouped by material class (tune.sort_shading) ------------------------------------
+// A class is what decides the shade kernel's control flow: a miss, a layered stack, or the type of a
+// single-layer BSDF.  The slots of an iteration are counted per class, the counts turned into
+// offsets, and the slot indices scattered into `order`, so the warps of k_shade take the paths of one
+// class together.  The order is only a permutation of slots: every path computes the same values.
+constexpr int kShadeClasses = 8;   // miss, layered, 4 single-layer BSDF types (+ 2 spare)
+
+__device__ __forceinline__ int shade_class(const Wave& W, const PathBuf& cur, const float4* hits, uint32_t i) {
+    const uint32_t prim = __float_as_uint(hits[i].y);
+    if (prim == SPT_MISS) return 0;
+    const PtJob& J = W.jobs[__float_as_uint(cur.b[i].w) >> 16];
+    const DevMaterial m = J.S.mat[J.S.prim_mat[prim]];
+    if (m.layer_count != 1) return 1;
+    return 2 + (J.S.bsdf[J.S.layer_ids[m.layer_begin]].type & 3);
+}
+
+// counts[k] += slots of class k (block-local histogram, one atomic per class per block)
+__global__ void __launch_bounds__(256) k_class_count(Wave W, const Counters* __restrict__ ctr, PathBuf cur,
+                                                     const float4* __restrict__ hits, uint32_t* counts) {
+    __shared__ uint32_t h[kShadeClasses];
+    if (threadIdx.x < kShadeClasses) h[threadIdx.x] = 0;
+    __syncthreads();
+    const Counters c = *ctr;
+    const uint32_t n = c.n_alive + n_new_paths(W, c);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        atomicAdd(&h[shade_class(W, cur, hits, i)], 1u);
+    __syncthreads();
+    if (threadIdx.x < kShadeClasses && h[threadIdx.x]) atomicAdd(&counts[threadIdx.x], h[threadIdx.x]);
+}
+
+// cursors[k] = counts[0] + ... + counts[k-1]; counts cleared for the next iteration
+__global__ void k_class_offsets(uint32_t* counts, uint32_t* cursors) {
+    uint32_t sum = 0;
+    for (int k = 0; k < kShadeClasses; ++k) {
+        cursors[k] = sum;
+        sum += counts[k];
+        counts[k] = 0;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_class_scatter(Wave W, const Counters* __restrict__ ctr, PathBuf cur,
+                                                       const float4* __restrict__ hits, uint32_t* cursors,
+                                                       uint32_t* __restrict__ order) {
+    const Counters c = *ctr;
+    const uint32_t n = c.n_alive + n_new_paths(W, c);
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t i = base + threadIdx.x;
+        const int k = i < n ? shade_class(W, cur, hits, i) : -1;
+        for (int q = 0; q < kShadeClasses; ++q) {   // warp-aggregated append per class
+            const unsigned mask = __ballot_sync(0xFFFFFFFFu, k == q);
+            if (!mask) continue;
+            uint32_t first = 0;
+            if (lane == __ffs(mask) - 1) first = atomicAdd(&cursors[q], static_cast<uint32_t>(__popc(mask)));
+            first = __shfl_sync(0xFFFFFFFFu, first, __ffs(mask) - 1);
+            if (k == q) order[first + __popc(mask & ((1u << lane) - 1u))] = i;
+        }
+    }
+}
+
 template <bool GUIDED>
 __global__ void __launch_bounds__(256) k_shade(Wave W, Counters* __restrict__ ctr, PathBuf cur, PathBuf nxt,
-                                               const float4* __restrict__ hits, GuideIO G) {
+                                               const float4* __restrict__ hits, GuideIO G,
+                                               const uint32_t* __restrict__ order) {
     const Counters c = *ctr;
     const uint32_t n = c.n_alive + n_new_paths(W, c);
     const uint32_t lane = threadIdx.x & 31;
     // all lanes of a warp iterate together so the append below can be warp-aggregated
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
+        const uint32_t j = base + threadIdx.x;
         bool keep = false;
         float4 wo_o, wo_d, wo_b, wo_l;
         uint4 rr = make_uint4(kNoRec, kNoRec, kNoRec, kNoRec);
-        if (i < n) {
+        if (j < n) {
+            const uint32_t i = order ? order[j] : j;   // the slot this lane shades
             const float4 o4 = cur.o[i], d4 = cur.d[i], b4 = cur.b[i], l4 = cur.l[i], h4 = hits[i];
             if (GUIDED) rr = cur.r[i];
             const uint32_t pix = __float_as_uint(o4.w), sg = __float_as_uint(d4.w);
@@ -455,6 +517,7 @@ spt_status make_job(spt_context* ctx, const spt_scene* sc, const spt_camera* cam
     J.npix = J.cam.vp_width * J.cam.vp_height;
     J.spp_offset = p->spp_offset;
     J.image = d_image;
+    J.layered = sc->any_layered ? 1u : 0u;
     set_sample_range(J, 0, J.spp);
     return SPT_OK;
 }
@@ -512,7 +575,9 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
     void* mem;
     const size_t buf_bytes = stride * sizeof(float4);
     const size_t job_bytes = jobs.size() * sizeof(PtJob);
-    if ((st = scratch(ctx, 5, buf_bytes * 9 + sizeof(Counters) + job_bytes + 512, &mem)) != SPT_OK) return st;
+    const size_t order_bytes = (stride * sizeof(uint32_t) + 255) & ~static_cast<size_t>(255);
+    if ((st = scratch(ctx, 5, buf_bytes * 9 + sizeof(Counters) + job_bytes + 512 + order_bytes + 256, &mem)) != SPT_OK)
+        return st;
     char* base = static_cast<char*>(mem);
     PathBuf A{reinterpret_cast<float4*>(base), reinterpret_cast<float4*>(base + buf_bytes),
               reinterpret_cast<float4*>(base + 2 * buf_bytes), reinterpret_cast<float4*>(base + 3 * buf_bytes), nullptr};
@@ -522,7 +587,15 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
     float4* hits = reinterpret_cast<float4*>(base + 8 * buf_bytes);
     Counters* d_ctr = reinterpret_cast<Counters*>(base + 9 * buf_bytes);
     PtJob* d_jobs = reinterpret_cast<PtJob*>(base + 9 * buf_bytes + 256);
+    char* tail = base + 9 * buf_bytes + 256 + ((job_bytes + 255) & ~static_cast<size_t>(255));
+    uint32_t* d_order = reinterpret_cast<uint32_t*>(tail);
+    uint32_t* d_class = reinterpret_cast<uint32_t*>(tail + order_bytes);   // counts[8], cursors[8]
+    bool any_layered = false;
+    for (const PtJob& J : jobs) any_layered |= J.layered != 0;
+    // measured: +8 % on the layered 1.3M-tri workload, -6 % on the box of Lambertian walls
+    const bool sort_shading = tune.sort_shading == 1 || (tune.sort_shading == 0 && any_layered);
     SPT_CUDA(ctx, cudaMemsetAsync(d_ctr, 0, sizeof(Counters), ctx->stream));
+    if (sort_shading) SPT_CUDA(ctx, cudaMemsetAsync(d_class, 0, 2 * kShadeClasses * sizeof(uint32_t), ctx->stream));
     SPT_CUDA(ctx, cudaMemcpyAsync(d_jobs, jobs.data(), job_bytes, cudaMemcpyHostToDevice, ctx->stream));
     GuideIO G{};
     uint32_t batch = 0, rec_cap = 0;
@@ -575,12 +648,19 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
         if (trav == 2) k_extend_df<<<g_df, 128, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
         else if (trav == 1) k_extend<1><<<g_ext, eb, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
         else k_extend<0><<<g_ext, eb, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
+        const uint32_t* order = nullptr;
+        if (sort_shading) {
+            k_class_count<<<g_shd, 256, 0, ctx->stream>>>(W, d_ctr, cur, hits, d_class);
+            k_class_offsets<<<1, 1, 0, ctx->stream>>>(d_class, d_class + kShadeClasses);
+            k_class_scatter<<<g_shd, 256, 0, ctx->stream>>>(W, d_ctr, cur, hits, d_class + kShadeClasses, d_order);
+            order = d_order;
+        }
         if (guide) {
             k_guide_collect<<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, hits, G);
             guide->infer_list(G.infer_in, &d_ctr->n_guided, static_cast<uint32_t>(cap), G.lobes, ctx->stream);
-            k_shade<true><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G);
+            k_shade<true><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
         } else {
-            k_shade<false><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G);
+            k_shade<false><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
         }
         k_advance<<<1, 1, 0, ctx->stream>>>(W, d_ctr);
     }

@@ -45,6 +45,7 @@ struct spt_scene {
     uint32_t tree_height = 0;
     uint32_t n_materials = 0;
     bool any_emission = false;
+    bool any_layered = false;      // a material with more than one BSDF layer
 };
 
 namespace spt {

@@ -33,9 +33,9 @@ def test_tuning_does_not_change_images(device):
     batch = _small_batch(3)
     jobs = [(spt.GpuScene(device, sb.build()), cam, p) for sb, cam, p, _ in batch]
     outs = []
-    for trav, cap, shade in ((2, 1 << 20, 128), (1, 4096, 64), (0, 100000, 256)):
+    for trav, cap, shade, srt in ((2, 1 << 20, 128, 2), (1, 4096, 64, 1), (0, 100000, 256, 0), (1, 1 << 20, 128, 1)):
         t = spt.default_tune()
-        t.traversal, t.capacity, t.shade_block = trav, cap, shade
+        t.traversal, t.capacity, t.shade_block, t.sort_shading = trav, cap, shade, srt
         bufs = [torch.zeros(c.height * c.width * 3, dtype=torch.float32, device="cuda") for _, c, _ in jobs]
         spt.render_batch(device, jobs, [b.data_ptr() for b in bufs], tune=t)
         outs.append([b.cpu().numpy() for b in bufs])
