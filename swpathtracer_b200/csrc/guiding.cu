@@ -47,10 +47,28 @@ __device__ __forceinline__ void stage_weights(const Model& M, __nv_bfloat16* sw,
 }
 
 // ---- inference --------------------------------------------------------------------------------
+// k_encode: the hash-grid features of n samples, one thread per (sample, level) so that every SM
+// keeps many gathers in flight; feats[16 i + l] = level l's two bf16 features of sample i.
+__global__ void __launch_bounds__(256) k_encode(const __grid_constant__ Model M, const float4* __restrict__ in,
+                                                uint32_t n_host, const uint32_t* __restrict__ n_dev,
+                                                uint32_t* __restrict__ feats) {
+    const uint32_t n = n_dev ? *n_dev : n_host;
+    const uint64_t total = static_cast<uint64_t>(n) * kLevels;
+    for (uint64_t t = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; t < total;
+         t += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint32_t i = static_cast<uint32_t>(t / kLevels), l = static_cast<uint32_t>(t % kLevels);
+        const V3 q = normalised_pos(M, f3v(__ldg(in + 3 * i)));
+        const __nv_bfloat162 f = encode_level(M, M.level[l], q, static_cast<int>(l));
+        feats[t] = *reinterpret_cast<const uint32_t*>(&f);
+    }
+}
+
 // in: n samples, 3 float4 each (position, normal, outgoing direction); out: 40 floats per sample
 // (8 lobes x {mu.xyz, kappa, weight}), already decoded.
+// feats: the k_encode output for the same samples.
 __global__ void __launch_bounds__(kInferWarps * 32) k_infer(Model M, const float4* __restrict__ in, uint32_t n_host,
-                                                            const uint32_t* __restrict__ n_dev, float* __restrict__ out) {
+                                                            const uint32_t* __restrict__ n_dev,
+                                                            const uint32_t* __restrict__ feats, float* __restrict__ out) {
     const uint32_t n = n_dev ? *n_dev : n_host;
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(smem);
@@ -63,7 +81,10 @@ __global__ void __launch_bounds__(kInferWarps * 32) k_infer(Model M, const float
         const uint32_t i = tile * kTileRows + lane;
         __nv_bfloat162* row = reinterpret_cast<__nv_bfloat162*>(xin + lane * pad(kIn));
         if (i < n) {
-            encode_inputs(M, f3v(in[3 * i]), f3v(in[3 * i + 1]), f3v(in[3 * i + 2]), row);
+            const uint4* f = reinterpret_cast<const uint4*>(feats + 16ull * i);
+            uint4* r4 = reinterpret_cast<uint4*>(row);
+            for (int k = 0; k < 4; ++k) r4[k] = __ldg(f + k);
+            direction_inputs(f3v(in[3 * i + 1]), f3v(in[3 * i + 2]), row);
         } else {
             for (int k = 0; k < kIn / 2; ++k) row[k] = __floats2bfloat162_rn(0.0f, 0.0f);
         }
@@ -447,24 +468,35 @@ spt_status Guide::refresh() {
     return SPT_OK;
 }
 
-spt_status Guide::infer(const float4* d_in, uint32_t n, float* d_out, cudaStream_t s) {
-    if (n == 0) return SPT_OK;
-    const uint32_t tiles = (n + kTileRows - 1) / kTileRows;
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((tiles + kInferWarps - 1) / kInferWarps, sms));
-    k_infer<<<grid, kInferWarps * 32, infer_smem_bytes(), s>>>(model, d_in, n, nullptr, d_out);
-    SPT_CUDA(ctx, cudaGetLastError());
+spt_status Guide::ensure_features(uint32_t n) {
+    if (n <= feats_cap) return SPT_OK;
+    if (feats) SPT_CUDA(ctx, cudaFree(feats));
+    feats = nullptr;
+    feats_cap = 0;
+    SPT_CUDA(ctx, cudaMalloc(&feats, static_cast<size_t>(n) * kLevels * sizeof(uint32_t)));
+    feats_cap = n;
     return SPT_OK;
 }
 
+spt_status Guide::infer(const float4* d_in, uint32_t n, float* d_out, cudaStream_t s) {
+    if (n == 0) return SPT_OK;
+    spt_status st = ensure_features(n);
+    if (st != SPT_OK) return st;
+    return infer_list(d_in, nullptr, n, d_out, s);
+}
+
 spt_status Guide::infer_list(const float4* d_in, const uint32_t* d_n, uint32_t max_n, float* d_out, cudaStream_t s) {
+    if (max_n > feats_cap) return fail(ctx, SPT_ERR_INTERNAL, "guide feature buffer smaller than the sample list");
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     const uint32_t tiles = (max_n + kTileRows - 1) / kTileRows;
+    const uint64_t pairs = static_cast<uint64_t>(max_n) * kLevels;
+    const unsigned g_enc = static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((pairs + 255) / 256, 16ull * sms)));
     const unsigned grid =
         static_cast<unsigned>(std::max<uint64_t>(1, std::min<uint64_t>((tiles + kInferWarps - 1) / kInferWarps, sms)));
-    k_infer<<<grid, kInferWarps * 32, infer_smem_bytes(), s>>>(model, d_in, 0, d_n, d_out);
+    const uint32_t n_host = d_n ? 0u : max_n;
+    k_encode<<<g_enc, 256, 0, s>>>(model, d_in, n_host, d_n, feats);
+    k_infer<<<grid, kInferWarps * 32, infer_smem_bytes(), s>>>(model, d_in, n_host, d_n, feats, d_out);
     SPT_CUDA(ctx, cudaGetLastError());
     return SPT_OK;
 }

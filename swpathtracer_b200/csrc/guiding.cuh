@@ -92,27 +92,34 @@ __device__ __forceinline__ Corner grid_corner(const GridLevel& lv, V3 q, int c) 
     return k;
 }
 
-// The 48 network inputs of one sample, as bf16 pairs: 32 grid features, normal, wo, zeros.
-__device__ __forceinline__ void encode_inputs(const Model& M, V3 pos, V3 nrm, V3 wo, __nv_bfloat162* row) {
-    const V3 q = normalised_pos(M, pos);
-#pragma unroll 2
-    for (int l = 0; l < kLevels; ++l) {
-        const GridLevel lv = M.level[l];
-        float a = 0.0f, b = 0.0f;
+// The two features of level l at the normalised position q (trilinear over the 8 cell corners).
+__device__ __forceinline__ __nv_bfloat162 encode_level(const Model& M, const GridLevel& lv, V3 q, int l) {
+    float a = 0.0f, b = 0.0f;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const Corner k = grid_corner(lv, q, c);
-            const __nv_bfloat162 f =
-                *reinterpret_cast<const __nv_bfloat162*>(M.grid + (static_cast<uint64_t>(l) * kT + k.idx) * kFeat);
-            a = __fmaf_rn(k.w, __bfloat162float(f.x), a);
-            b = __fmaf_rn(k.w, __bfloat162float(f.y), b);
-        }
-        row[l] = __floats2bfloat162_rn(a, b);
+    for (int c = 0; c < 8; ++c) {
+        const Corner k = grid_corner(lv, q, c);
+        const __nv_bfloat162 f =
+            *reinterpret_cast<const __nv_bfloat162*>(M.grid + (static_cast<uint64_t>(l) * kT + k.idx) * kFeat);
+        a = __fmaf_rn(k.w, __bfloat162float(f.x), a);
+        b = __fmaf_rn(k.w, __bfloat162float(f.y), b);
     }
+    return __floats2bfloat162_rn(a, b);
+}
+
+// The 16 network inputs after the grid features: normal, wo, zeros.
+__device__ __forceinline__ void direction_inputs(V3 nrm, V3 wo, __nv_bfloat162* row) {
     row[16] = __floats2bfloat162_rn(nrm.x, nrm.y);
     row[17] = __floats2bfloat162_rn(nrm.z, wo.x);
     row[18] = __floats2bfloat162_rn(wo.y, wo.z);
     for (int i = 19; i < kIn / 2; ++i) row[i] = __floats2bfloat162_rn(0.0f, 0.0f);
+}
+
+// The 48 network inputs of one sample, as bf16 pairs: 32 grid features, normal, wo, zeros.
+__device__ __forceinline__ void encode_inputs(const Model& M, V3 pos, V3 nrm, V3 wo, __nv_bfloat162* row) {
+    const V3 q = normalised_pos(M, pos);
+#pragma unroll 2
+    for (int l = 0; l < kLevels; ++l) row[l] = encode_level(M, M.level[l], q, l);
+    direction_inputs(nrm, wo, row);
 }
 
 // ---- warp-level MMA --------------------------------------------------------------------------

@@ -29,16 +29,22 @@ struct Guide {
     float* partial = nullptr;
     uint32_t train_cap = 0;
     std::vector<void*> train_allocs;
+    // inference scratch: the hash-grid features of up to feats_cap samples (k_encode -> k_infer)
+    uint32_t* feats = nullptr;
+    uint32_t feats_cap = 0;
 
     spt_status alloc(spt_context* c, const spt_guide_config& cfg);
     spt_status refresh();
     spt_status infer(const float4* d_in, uint32_t n, float* d_out, cudaStream_t s);
     // inference for a device-side count of samples (at most max_n); usable inside a CUDA graph
+    // (ensure_features(max_n) first, outside any stream capture)
     spt_status infer_list(const float4* d_in, const uint32_t* d_n, uint32_t max_n, float* d_out, cudaStream_t s);
+    spt_status ensure_features(uint32_t n);
     spt_status ensure_train_buffers(uint32_t n);
     spt_status gradients(const float4* d_rec, uint32_t n);
     spt_status step(const float4* d_rec, uint32_t n, float* loss);
     ~Guide() {
+        if (feats) cudaFree(feats);
         for (void* p : train_allocs) cudaFree(p);
         for (void* p : allocations) cudaFree(p);
     }

@@ -621,6 +621,7 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
         G.recx = G.rec + 4ull * rec_cap;
         G.mix = guide->cfg.mix;
         G.rec_cap = rec_cap;
+        if ((st = guide->ensure_features(static_cast<uint32_t>(cap))) != SPT_OK) return st;
         const uint32_t on = train_budget > 0 ? 1u : 0u;
         SPT_CUDA(ctx, cudaMemcpyAsync(&d_ctr->train_on, &on, sizeof(on), cudaMemcpyHostToDevice, ctx->stream));
         SPT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
