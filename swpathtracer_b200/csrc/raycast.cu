@@ -229,7 +229,7 @@ static spt_status launch_raycast(spt_context* ctx, const spt_scene* sc, const De
 namespace spt {
 namespace {
 
-constexpr uint64_t kPipeChunk = 1ull << 21;  // rays per pipeline chunk (64 MB in, 32 MB out)
+constexpr uint64_t kPipeChunk = 1ull << 20;  // rays per pipeline chunk (32 MB in, 16 MB out)
 
 bool is_pinned(const void* p) {
     cudaPointerAttributes a;

@@ -21,7 +21,7 @@ struct spt_context {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // streams of the chunked host-buffer pipeline (spt_intersect): copies in, queries and copies out
     // of successive chunks overlap; ev_pipe[i] orders a chunk after the previous user of its buffers
-    static constexpr int kPipe = 3;
+    static constexpr int kPipe = 4;
     cudaStream_t pipe[kPipe] = {};
     cudaEvent_t ev_pipe[kPipe] = {};
     uint32_t* d_status = nullptr;  // device error word: bit 0 stack overflow, bit 1 queue overflow, bit 2 timeout

@@ -115,12 +115,12 @@ def test_full_size_mesh_closest_equals_exhaustive(device):
 
 
 def test_pipelined_host_queries_match_device_queries(device):
-    """spt_intersect with page-locked host buffers runs in chunks over three streams; the hits and
+    """spt_intersect with page-locked host buffers runs in chunks over four streams; the hits and
     counts equal one device-side query of the whole batch (and the pageable path)."""
     import torch
     packed = scenes.displaced_mesh_scene(6).build()
     gs = spt.GpuScene(device, packed)
-    n = (1 << 21) * 2 + 12345                   # three chunks, the last one partial
+    n = (1 << 21) * 2 + 12345                   # five chunks of 2^20, the last one partial
     rays = scenes.incoherent_rays(n, seed=77, half_extent=1.5)
     h_rays = torch.from_numpy(rays).pin_memory()
     h_hits = torch.empty((n, 4), dtype=torch.int32).pin_memory().numpy().view(abi.HIT_DTYPE).reshape(n)
