@@ -108,7 +108,9 @@ def cpu_baseline(packed, rays_np, budget_rays):
         from oracle.bindings import RefHarness
         h = RefHarness()
         kind = "reference"
+        t0 = time.perf_counter()
         rs = h.scene(packed, n_threads=cores)
+        ref_build_s = time.perf_counter() - t0
         r = rs.intersect(sample, n_threads=cores, want_normals=False)
         secs = r["seconds"]
     except FileNotFoundError:
@@ -118,8 +120,11 @@ def cpu_baseline(packed, rays_np, budget_rays):
         t0 = time.perf_counter()
         osc.intersect(sample, n_threads=cores, want_normals=False)
         secs = time.perf_counter() - t0
-    return {"value": round(len(sample) / secs / 1e6, 4), "unit": "Mrays/s", "cores": cores, "kind": kind,
-            "sample": "%d of the step's incoherent rays, SBVH::intersect per ray, OpenMP over rays" % len(sample)}
+    out = {"value": round(len(sample) / secs / 1e6, 4), "unit": "Mrays/s", "cores": cores, "kind": kind,
+           "sample": "%d of the step's incoherent rays, SBVH::intersect per ray, OpenMP over rays" % len(sample)}
+    if kind == "reference":
+        out["sbvh_build_s"] = round(ref_build_s, 2)   # SBVH::build, single-threaded in the reference
+    return out
 
 
 def guided_vs_plain(spt, scenes, dev, torch, spp=4096):
@@ -246,7 +251,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     packed = build_scene(a.subdiv)
+    t_build = time.perf_counter()
     bvh = spt.Bvh(packed)
+    build_ms = (time.perf_counter() - t_build) * 1e3
     dev = spt.Device(local)
     gs = spt.GpuScene(dev, packed, bvh)
     n = 1 << a.rays_log2
@@ -329,6 +336,7 @@ def main():
            "e2e": {"value": round(e2e, 3), "unit": "Mrays/s", "h2d_bytes_per_step": n * 32,
                    "d2h_bytes_per_step": n * 16},
            "gpu_launches": a.steps,
+           "bvh_build_ms": round(build_ms, 1),
            "clocks": clk}
 
     if rank == 0 and not a.no_extras:
