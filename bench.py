@@ -127,15 +127,15 @@ def cpu_baseline(packed, rays_np, budget_rays):
     return out
 
 
-def guided_vs_plain(spt, scenes, dev, torch, spp=4096):
-    """Equal-time relMSE of guided vs plain path tracing on the small-light box (128^2, max length 5;
-    the light is a 0.06 x 0.06 quad, found only by sampling its direction).  Both render `spp`
-    samples; each image's relMSE mean((I - R)^2 / (R^2 + 1e-2)) against a 16,384-spp plain render
-    is multiplied by its wall time (relMSE falls as 1/time), and the ratio plain / guided of those
-    products is the relMSE ratio at equal time (> 1: guiding wins).  The guided time includes its
-    online training (256 Adam steps of 2^16 records)."""
+def guided_vs_plain(spt, scenes, dev, torch, name, sb, spp, ref_spp, steps, seeds=(7, 8)):
+    """Equal-time relMSE of guided vs plain path tracing (128^2, max length 5).  Plain and guided both
+    render `spp` samples per seed; each image's relMSE mean((I - R)^2 / (R^2 + 1e-2)) against a
+    `ref_spp` plain render is multiplied by its wall time (relMSE falls as 1/time), and the ratio
+    plain / guided of the products, summed over the seeds, is the relMSE ratio at equal time
+    (> 1: guiding wins).  The guided time includes the guide's online training (`steps` Adam steps of
+    2^16 records, mix 0.5) and its lobe-cache refreshes; each seed trains a fresh guide."""
     import numpy as np
-    gs = spt.GpuScene(dev, scenes.small_light_box_scene().build())
+    gs = spt.GpuScene(dev, sb.build())
     cam = scenes.box_camera(128, 128)
     img = torch.empty(128 * 128 * 3, dtype=torch.float32, device="cuda")
 
@@ -154,17 +154,20 @@ def guided_vs_plain(spt, scenes, dev, torch, spp=4096):
         return float(np.mean((a - b) ** 2 / (b ** 2 + 1e-2)))
 
     render(64, 1)
-    ref, _ = render(16384, 99)
-    plain, t_plain = render(spp, 7)
-    g = spt.Guide(dev, spt.guide_config(batch=1 << 16, max_steps=256, mix=0.5, seed=1))
-    guided, t_guided = render(spp, 7, g)
-    e_plain, e_guided = relmse(plain, ref), relmse(guided, ref)
-    g.close()
+    ref, _ = render(ref_spp, 99)
+    ep = eg = tp = tg = 0.0
+    for seed in seeds:
+        plain, t = render(spp, seed)
+        ep, tp = ep + relmse(plain, ref), tp + t
+        g = spt.Guide(dev, spt.guide_config(batch=1 << 16, max_steps=steps, mix=0.5, seed=seed))
+        guided, t = render(spp, seed, g)
+        eg, tg = eg + relmse(guided, ref), tg + t
+        g.close()
     gs.close()
-    return {"guided_small_light_128x128_spp": spp,
-            "guided_relmse_plain": round(e_plain, 5), "guided_relmse_guided": round(e_guided, 5),
-            "guided_wall_ms_plain": round(1e3 * t_plain, 2), "guided_wall_ms_guided": round(1e3 * t_guided, 2),
-            "guided_equal_time_relmse_ratio_plain_over_guided": round((e_plain * t_plain) / (e_guided * t_guided), 4)}
+    k = len(seeds)
+    return {name + "_spp": spp, name + "_relmse_plain": round(ep / k, 6), name + "_relmse_guided": round(eg / k, 6),
+            name + "_wall_ms_plain": round(1e3 * tp / k, 2), name + "_wall_ms_guided": round(1e3 * tg / k, 2),
+            name + "_equal_time_relmse_ratio_plain_over_guided": round((ep * tp) / (eg * tg), 4)}
 
 
 def cpu_pathtrace_baseline(subdiv):
@@ -389,7 +392,12 @@ def main():
         extras["batch64_paths"] = paths
         for g_, _, _ in jobs:
             g_.close()
-        extras.update(guided_vs_plain(spt, scenes, dev, torch))
+        # guided rendering: a room lit through a 0.1 x 0.1 window (directional transport), and the
+        # small-light box (light found mostly via a two-sided emitter's halo; guiding loses there)
+        extras.update(guided_vs_plain(spt, scenes, dev, torch, "guided_window_room_128x128",
+                                      scenes.window_room_scene(0.1), 16384, 262144, 32))
+        extras.update(guided_vs_plain(spt, scenes, dev, torch, "guided_small_light_128x128",
+                                      scenes.small_light_box_scene(), 4096, 16384, 32, seeds=(7,)))
         out["submetrics"] = extras
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(packed, rays_np, 1 << 22)

@@ -15,7 +15,8 @@ Model (all constants mirror csrc/guiding.cuh):
   * output lobe k of 8: mu = normalize(y[5k:5k+3]), kappa = exp(clamp(y[5k+3], -2.3, 7)),
     weights = softmax(y[5k+4]); vMF pdf kappa / (2 pi (1 - e^{-2 kappa})) e^{kappa (mu.w - 1)}.
   * loss per record: -c * log q(w), c = the record's normalised weight; batch loss = mean.
-  * Adam (beta1 0.9, beta2 0.99, eps 1e-15, bias-corrected).
+  * Adam (beta1 0.9, beta2 0.99, eps 1e-15, bias-corrected); for the hash grid the lazy form:
+    entries with a zero gradient keep their parameter and moments (adam_lazy).
 BF16: the kernels round the MLP inputs of every layer and the weights to bf16 and accumulate in
 fp32; bf16() below reproduces the rounding so the forward can be compared tightly.
 """
@@ -165,6 +166,13 @@ def grid_grad(corners, gfeat, shape):
         for idx, w in corners[l]:
             np.add.at(gt[l], idx, w[:, None] * gfeat[:, l * F:(l + 1) * F])
     return gt
+
+
+def adam_lazy(p, g, m, v, step, lr=1e-2, b1=0.9, b2=0.99, eps=1e-15):
+    """Adam where only entries with a nonzero gradient move (the hash grid's update)."""
+    p2, m2, v2 = adam(p, g, m, v, step, lr, b1, b2, eps)
+    touched = g != 0
+    return np.where(touched, p2, p), np.where(touched, m2, m), np.where(touched, v2, v)
 
 
 def adam(p, g, m, v, step, lr=1e-2, b1=0.9, b2=0.99, eps=1e-15):

@@ -65,6 +65,25 @@ __global__ void __launch_bounds__(256) k_encode(const __grid_constant__ Model M,
 
 // in: n samples, 3 float4 each (position, normal, outgoing direction); out: 40 floats per sample
 // (8 lobes x {mu.xyz, kappa, weight}), already decoded.
+// The network inputs of the guide cache: entry ((iz * R + iy) * R + ix) * 6 + bin is the centre of
+// cell (ix, iy, iz) of an R^3 grid over the box, with the normal +x, -x, +y, -y, +z, -z for bin 0..5
+// (wo = the normal).
+__global__ void k_cache_inputs(Model M, uint32_t R, float4* __restrict__ in) {
+    const uint32_t n = R * R * R * 6;
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const uint32_t bin = e % 6, cell = e / 6;
+        const uint32_t ix = cell % R, iy = (cell / R) % R, iz = cell / (R * R);
+        const float x = M.lo[0] + (ix + 0.5f) / (R * M.inv_ext[0]);
+        const float y = M.lo[1] + (iy + 0.5f) / (R * M.inv_ext[1]);
+        const float z = M.lo[2] + (iz + 0.5f) / (R * M.inv_ext[2]);
+        const float sgn = (bin & 1u) ? -1.0f : 1.0f;
+        const float4 nrm = make_float4(bin < 2 ? sgn : 0.0f, (bin >> 1) == 1 ? sgn : 0.0f, bin >= 4 ? sgn : 0.0f, 0.0f);
+        in[3 * e] = make_float4(x, y, z, 0.0f);
+        in[3 * e + 1] = nrm;
+        in[3 * e + 2] = nrm;
+    }
+}
+
 // feats: the k_encode output for the same samples.
 __global__ void __launch_bounds__(kInferWarps * 32) k_infer(Model M, const float4* __restrict__ in, uint32_t n_host,
                                                             const uint32_t* __restrict__ n_dev,
@@ -372,6 +391,27 @@ __global__ void k_adam(float* __restrict__ p, float* __restrict__ m, float* __re
     }
 }
 
+// Lazy Adam for the hash grid: an entry the batch did not touch (gradient exactly 0) keeps its
+// parameter and moments, so a step reads 4 bytes per untouched entry instead of updating all
+// 16.8M (the full update moved 571 MB per step).  Touched entries get the same update as k_adam.
+__global__ void k_adam_sparse(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v,
+                              float* __restrict__ g, __nv_bfloat16* __restrict__ copy, uint64_t n, float lr, float c1,
+                              float c2) {
+    for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const float gi = g[i];
+        if (gi == 0.0f) continue;
+        const float mi = 0.9f * m[i] + 0.1f * gi;
+        const float vi = 0.99f * v[i] + 0.01f * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + 1e-15f);
+        p[i] = pi;
+        g[i] = 0.0f;
+        copy[i] = __float2bfloat16_rn(pi);
+    }
+}
+
 __global__ void k_to_bf16(const float* __restrict__ p, __nv_bfloat16* __restrict__ q, uint64_t n) {
     for (uint64_t i = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
@@ -457,6 +497,13 @@ spt_status Guide::alloc(spt_context* c, const spt_guide_config& cfg_) {
     }
     model.grid = grid_bf16;
     model.smem_image = smem_image;
+    // everything a guided render needs is allocated here, so renders and training steps allocate
+    // nothing: the training buffers of one batch, the lobe cache and its inference scratch
+    if ((st = ensure_train_buffers(cfg.batch)) != SPT_OK) return st;
+    const uint32_t n_cache = cache_res * cache_res * cache_res * 6;
+    if ((st = ensure_features(n_cache)) != SPT_OK) return st;
+    SPT_CUDA(ctx, cudaMalloc(&cache, static_cast<size_t>(n_cache) * kOutUsed * sizeof(float)));
+    SPT_CUDA(ctx, cudaMalloc(&cache_in, static_cast<size_t>(n_cache) * 3 * sizeof(float4)));
     return refresh();
 }
 
@@ -476,6 +523,17 @@ spt_status Guide::ensure_features(uint32_t n) {
     SPT_CUDA(ctx, cudaMalloc(&feats, static_cast<size_t>(n) * kLevels * sizeof(uint32_t)));
     feats_cap = n;
     return SPT_OK;
+}
+
+spt_status Guide::refresh_cache() {
+    const uint32_t n = cache_res * cache_res * cache_res * 6;
+    if (!cache) {
+        SPT_CUDA(ctx, cudaMalloc(&cache, static_cast<size_t>(n) * kOutUsed * sizeof(float)));
+        SPT_CUDA(ctx, cudaMalloc(&cache_in, static_cast<size_t>(n) * 3 * sizeof(float4)));
+    }
+    k_cache_inputs<<<256, 256, 0, ctx->stream>>>(model, cache_res, cache_in);
+    SPT_CUDA(ctx, cudaGetLastError());
+    return infer(cache_in, n, cache, ctx->stream);
 }
 
 spt_status Guide::infer(const float4* d_in, uint32_t n, float* d_out, cudaStream_t s) {
@@ -563,7 +621,8 @@ spt_status Guide::step(const float4* d_rec, uint32_t n, float* loss) {
     ++steps;
     const float c1 = 1.0f - std::pow(0.9f, static_cast<float>(steps));
     const float c2 = 1.0f - std::pow(0.99f, static_cast<float>(steps));
-    k_adam<<<4096, 256, 0, ctx->stream>>>(grid_master, grid_m, grid_v, grid_grad, grid_bf16, kGridParams, cfg.lr, c1, c2);
+    k_adam_sparse<<<4096, 256, 0, ctx->stream>>>(grid_master, grid_m, grid_v, grid_grad, grid_bf16, kGridParams, cfg.lr,
+                                                 c1, c2);
     k_adam<<<72, 256, 0, ctx->stream>>>(mlp_master, mlp_m, mlp_v, mlp_grad, nullptr, kMlpParams, cfg.lr, c1, c2);
     k_stage<<<(kMlpParams + 255) / 256, 256, 0, ctx->stream>>>(mlp_master, smem_image);
     SPT_CUDA(ctx, cudaGetLastError());

@@ -32,6 +32,12 @@ struct Guide {
     // inference scratch: the hash-grid features of up to feats_cap samples (k_encode -> k_infer)
     uint32_t* feats = nullptr;
     uint32_t feats_cap = 0;
+    // the mixture cached per (cell of a cache_res^3 grid over the box, normal axis): what guided
+    // rendering samples, refreshed after every round of training
+    static constexpr uint32_t kCacheRes = 32;
+    uint32_t cache_res = kCacheRes;
+    float* cache = nullptr;        // kCacheRes^3 * 6 * 40 floats
+    float4* cache_in = nullptr;    // the network inputs of the cache entries
 
     spt_status alloc(spt_context* c, const spt_guide_config& cfg);
     spt_status refresh();
@@ -40,11 +46,14 @@ struct Guide {
     // (ensure_features(max_n) first, outside any stream capture)
     spt_status infer_list(const float4* d_in, const uint32_t* d_n, uint32_t max_n, float* d_out, cudaStream_t s);
     spt_status ensure_features(uint32_t n);
+    spt_status refresh_cache();
     spt_status ensure_train_buffers(uint32_t n);
     spt_status gradients(const float4* d_rec, uint32_t n);
     spt_status step(const float4* d_rec, uint32_t n, float* loss);
     ~Guide() {
         if (feats) cudaFree(feats);
+        if (cache) cudaFree(cache);
+        if (cache_in) cudaFree(cache_in);
         for (void* p : train_allocs) cudaFree(p);
         for (void* p : allocations) cudaFree(p);
     }

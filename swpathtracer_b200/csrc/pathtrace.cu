@@ -56,7 +56,7 @@ struct Counters {
     uint32_t n_alive;               // live slots at the start of the iteration (in the current buffer)
     uint32_t n_next;                // slots appended to the other buffer by k_shade
     uint32_t iterations;
-    uint32_t n_guided;              // guided renders: hits listed for the guide this iteration
+    uint32_t spare;
     uint32_t rec_count;             // training records written into the current generation
     uint32_t rec_gen;               // generation of the record buffer (bumped when it is consumed)
     uint32_t train_on;              // record training data
@@ -68,9 +68,9 @@ struct Counters {
 struct GuideIO {
     float mix;
     uint32_t rec_cap;
-    float4* infer_in;      // 3 float4 per listed hit: position, normal, outgoing direction
-    float* lobes;          // 40 floats per listed hit
-    uint32_t* slot_list;   // slot -> list index, or ~0
+    const float* cache;    // the guide's mixture per (position cell, normal axis): 40 floats each
+    uint32_t cache_res;    // cells per axis over the guide's box
+    float lo[3], inv_ext[3];
     float4* rec;           // 4 float4 per record (spt_guide_record layout)
     float4* recx;          // 2 float4 per record: throughput at the record, radiance gathered after it
 };
@@ -139,48 +139,20 @@ __global__ void __launch_bounds__(256) k_generate(Wave W, const Counters* __rest
     }
 }
 
-// Guided renders: list this iteration's hits on guidable materials and the guide's inputs for them.
-__global__ void __launch_bounds__(256) k_guide_collect(Wave W, Counters* __restrict__ ctr, PathBuf cur,
-                                                      const float4* __restrict__ hits, GuideIO G) {
-    const Counters c = *ctr;
-    const uint32_t n = c.n_alive + n_new_paths(W, c);
-    const uint32_t lane = threadIdx.x & 31;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
-        bool take = false;
-        float4 p4, n4, w4;
-        if (i < n) {
-            const float4 h4 = hits[i];
-            const uint32_t prim = __float_as_uint(h4.y);
-            if (prim != SPT_MISS) {
-                const PtJob& J = W.jobs[__float_as_uint(cur.b[i].w) >> 16];
-                const DevMaterial m = J.S.mat[J.S.prim_mat[prim]];
-                if (guidable(J.S, m)) {
-                    const V3 o = f3v(cur.o[i]), d = f3v(cur.d[i]);
-                    const V3 pos = hit_pos(J.S.prim_type[prim] == SPT_PRIM_SPHERE, o, d, h4.x);
-                    const V3 nrm = hit_normal(J.S, prim, h4.z, h4.w, pos);
-                    p4 = make_float4(pos.x, pos.y, pos.z, 0.0f);
-                    n4 = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
-                    w4 = make_float4(-d.x, -d.y, -d.z, 0.0f);
-                    take = true;
-                }
-            }
-            if (!take) G.slot_list[i] = kNoRec;
-        }
-        const unsigned mask = __ballot_sync(0xFFFFFFFFu, take);
-        if (mask) {
-            uint32_t first = 0;
-            if (lane == 0) first = atomicAdd(&ctr->n_guided, static_cast<uint32_t>(__popc(mask)));
-            first = __shfl_sync(0xFFFFFFFFu, first, 0);
-            if (take) {
-                const uint32_t k = first + __popc(mask & ((1u << lane) - 1u));
-                G.slot_list[i] = k;
-                G.infer_in[3 * k] = p4;
-                G.infer_in[3 * k + 1] = n4;
-                G.infer_in[3 * k + 2] = w4;
-            }
-        }
-    }
+// The guide's cache entry of a surface point: its cell in a cache_res^3 grid over the guide's box and
+// the axis (with sign) its normal is closest to.
+__device__ __forceinline__ uint32_t cache_cell(const GuideIO& G, V3 pos, V3 nrm) {
+    const float hi = 0.99999994f;
+    const float qx = fminf(fmaxf((pos.x - G.lo[0]) * G.inv_ext[0], 0.0f), hi);
+    const float qy = fminf(fmaxf((pos.y - G.lo[1]) * G.inv_ext[1], 0.0f), hi);
+    const float qz = fminf(fmaxf((pos.z - G.lo[2]) * G.inv_ext[2], 0.0f), hi);
+    const uint32_t r = G.cache_res;
+    const uint32_t ix = static_cast<uint32_t>(qx * r), iy = static_cast<uint32_t>(qy * r), iz = static_cast<uint32_t>(qz * r);
+    const float ax = fabsf(nrm.x), ay = fabsf(nrm.y), az = fabsf(nrm.z);
+    const uint32_t bin = (ax >= ay && ax >= az) ? (nrm.x < 0.0f ? 1u : 0u)
+                         : (ay >= az)           ? (nrm.y < 0.0f ? 3u : 2u)
+                                                : (nrm.z < 0.0f ? 5u : 4u);
+    return ((iz * r + iy) * r + ix) * 6u + bin;
 }
 
 __device__ __forceinline__ float4 hit_record(const DevScene& S, const Hit1& h) {
@@ -361,9 +333,9 @@ __global__ void __launch_bounds__(256) k_shade(Wave W, Counters* __restrict__ ct
                 Stream bs(J.seed, path, static_cast<uint32_t>(depth) + 1u);
                 V3 f, refl, wi, wwi;
                 float pdf;
-                const uint32_t gi = GUIDED ? G.slot_list[i] : kNoRec;
+                const uint32_t gi = (GUIDED && guidable(J.S, m)) ? cache_cell(G, pos, nrm) : kNoRec;
                 if (GUIDED && gi != kNoRec) {
-                    const GuidedSample gs = guided_sample(J.S, m, frame, wo, G.lobes + 40ull * gi, G.mix, bs);
+                    const GuidedSample gs = guided_sample(J.S, m, frame, wo, G.cache + 40ull * gi, G.mix, bs);
                     f = gs.f;
                     refl = gs.refl;
                     wi = gs.wi_local;
@@ -456,7 +428,6 @@ __global__ void k_advance(Wave W, Counters* ctr) {
     c.n_alive = c.n_next;
     c.n_next = 0;
     c.fetch = 0;
-    c.n_guided = 0;
     c.iterations += 1;
     *ctr = c;
 }
@@ -605,22 +576,22 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
             return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "guide batch must be at most 2^22 records");
         rec_cap = kRecBatches * batch;
         void* gm;
-        const size_t gbytes = 2 * stride * sizeof(uint4) +
-                              stride * (3 * sizeof(float4) + 40 * sizeof(float) + sizeof(uint32_t)) +
-                              static_cast<size_t>(rec_cap) * 6 * sizeof(float4) + 1024;
+        const size_t gbytes = 2 * stride * sizeof(uint4) + static_cast<size_t>(rec_cap) * 6 * sizeof(float4) + 1024;
         if ((st = scratch(ctx, 2, gbytes, &gm)) != SPT_OK) return st;
         char* g = static_cast<char*>(gm);
         A.r = reinterpret_cast<uint4*>(g);
         B.r = A.r + stride;
-        G.infer_in = reinterpret_cast<float4*>(B.r + stride);
-        G.lobes = reinterpret_cast<float*>(G.infer_in + 3 * stride);
-        G.slot_list = reinterpret_cast<uint32_t*>(G.lobes + 40 * stride);
-        G.rec = reinterpret_cast<float4*>(reinterpret_cast<char*>(G.slot_list + stride) + 256 -
-                                          (reinterpret_cast<uintptr_t>(G.slot_list + stride) & 255));
+        G.rec = reinterpret_cast<float4*>(B.r + stride);
         G.recx = G.rec + 4ull * rec_cap;
         G.mix = guide->cfg.mix;
         G.rec_cap = rec_cap;
-        if ((st = guide->ensure_features(static_cast<uint32_t>(cap))) != SPT_OK) return st;
+        if ((st = guide->refresh_cache()) != SPT_OK) return st;
+        G.cache = guide->cache;
+        G.cache_res = guide->cache_res;
+        for (int k = 0; k < 3; ++k) {
+            G.lo[k] = guide->model.lo[k];
+            G.inv_ext[k] = guide->model.inv_ext[k];
+        }
         const uint32_t on = train_budget > 0 ? 1u : 0u;
         SPT_CUDA(ctx, cudaMemcpyAsync(&d_ctr->train_on, &on, sizeof(on), cudaMemcpyHostToDevice, ctx->stream));
         SPT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -656,8 +627,6 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
             order = d_order;
         }
         if (guide) {
-            k_guide_collect<<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, hits, G);
-            guide->infer_list(G.infer_in, &d_ctr->n_guided, static_cast<uint32_t>(cap), G.lobes, ctx->stream);
             k_shade<true><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
         } else {
             k_shade<false><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
@@ -693,6 +662,8 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
                 ++steps;
             }
         training = steps < train_budget;
+        spt_status s3 = guide->refresh_cache();   // the next iterations sample the updated guide
+        if (s3 != SPT_OK) return s3;
         k_next_generation<<<1, 1, 0, ctx->stream>>>(d_ctr, training ? 1u : 0u);
         return SPT_OK;
     };

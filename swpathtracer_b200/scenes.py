@@ -387,6 +387,37 @@ def small_light_box_scene(subdivisions=4, light_size=0.06):
     return sb
 
 
+def window_room_scene(window=0.1, subdivisions=4):
+    """Path guiding workload: a room lit only through a square window.  The open unit box of the box
+    scene, its right wall (x = 1) pierced by a window of side `window` centred at (y, z) = (0.6, 0.5),
+    and outside it a 2 x 2 emitter of radiance 20 at x = 1.6 facing the room, plus a Lambertian
+    sphere.  A path reaches the light only through the window, a small solid angle from most of the
+    room: the directional case where a learned sampling distribution pays."""
+    sb = SceneBuilder(background=(0.0, 0.0, 0.0))
+    grey = sb.material(sb.layered_bsdf(sb.lambertian(kd=WALL_COLOURS[0])))
+    red = sb.material(sb.layered_bsdf(sb.lambertian(kd=WALL_COLOURS[1])))
+    light = sb.material(sb.layered_bsdf(sb.lambertian(kd=(0.0, 0.0, 0.0))), emission=(20.0, 20.0, 20.0))
+    tris, mats = [], []
+
+    def quad(a, b, c, d, m):
+        tris.extend([[a, b, c], [a, c, d]])
+        mats.extend([m, m])
+    quad([0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], grey)          # back
+    quad([0, 0, 1], [1, 0, 1], [1, 0, 0], [0, 0, 0], grey)          # floor
+    quad([0, 1, 0], [1, 1, 0], [1, 1, 1], [0, 1, 1], grey)          # ceiling
+    quad([0, 0, 1], [0, 0, 0], [0, 1, 0], [0, 1, 1], red)           # left
+    zlo, zhi, ylo, yhi = 0.5 - window / 2, 0.5 + window / 2, 0.6 - window / 2, 0.6 + window / 2
+    quad([1, 0, 0], [1, 0, 1], [1, ylo, 1], [1, ylo, 0], grey)      # right wall around the window
+    quad([1, yhi, 0], [1, yhi, 1], [1, 1, 1], [1, 1, 0], grey)
+    quad([1, ylo, 0], [1, ylo, zlo], [1, yhi, zlo], [1, yhi, 0], grey)
+    quad([1, ylo, zhi], [1, ylo, 1], [1, yhi, 1], [1, yhi, zhi], grey)
+    quad([1.6, -0.5, -0.5], [1.6, 1.5, -0.5], [1.6, 1.5, 1.5], [1.6, -0.5, 1.5], light)
+    sb.triangles(np.array(tris, np.float32), np.array(mats, np.uint32))
+    diffuse = sb.material(sb.layered_bsdf(sb.lambertian(kd=(0.8, 0.8, 0.8))))
+    sb.triangles(displaced_icosphere(subdivisions, radius=0.2, center=(0.4, 0.2, 0.5), amplitude=0.0), diffuse)
+    return sb
+
+
 def layered_box_scene(subdivisions=8, seed=1):
     """Full path tracing at 1.3M tris: the displaced mesh (radius 1) inside the open box scaled x3,
     mesh material = LayeredBSDF{SmoothDielectric{ior 1.5}, CookTorrance{roughness 0.2}}."""

@@ -102,6 +102,22 @@ def test_adam_step_matches_oracle(device):
     g.close()
 
 
+def test_grid_adam_is_lazy(device):
+    """The hash grid's Adam step moves exactly the entries the batch touched, by the Adam update."""
+    g, grid, mlp = _guide(device, seed=11)
+    rng = np.random.default_rng(12)
+    recs = _records(rng, 512)
+    ggrid, _, _ = g.gradients(recs)
+    g.train(recs)
+    grid1, _ = g.get_params()
+    exp, _, _ = G.adam_lazy(grid.astype(np.float64), ggrid.astype(np.float64), 0.0, 0.0, 1)
+    touched = ggrid != 0
+    assert 0 < touched.sum() < touched.size // 10
+    np.testing.assert_array_equal(grid1[~touched], grid[~touched])
+    np.testing.assert_allclose(grid1[touched], exp[touched], rtol=1e-4, atol=1e-6)
+    g.close()
+
+
 def test_training_learns_a_directional_distribution(device):
     """Records whose incident directions cluster around a position-dependent direction: the loss
     falls and the learned mixture puts far more density there than uniform (1/4pi)."""
