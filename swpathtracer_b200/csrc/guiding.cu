@@ -84,6 +84,21 @@ __global__ void k_cache_inputs(Model M, uint32_t R, float4* __restrict__ in) {
     }
 }
 
+// Decoded lobes {mu.xyz, kappa, w} -> cache entries {mu.xyz, kappa, w, w * C(kappa)} (guiding.cuh).
+__global__ void k_cache_pack(const float* __restrict__ raw, uint32_t n, float* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n * kLobes; i += gridDim.x * blockDim.x) {
+        const float* l = raw + 5ull * i;
+        float* o = out + static_cast<uint64_t>(kCacheLobe) * i;
+        const float kappa = l[3];
+        o[0] = l[0];
+        o[1] = l[1];
+        o[2] = l[2];
+        o[3] = kappa;
+        o[4] = l[4];
+        o[5] = l[4] * (kappa / (2.0f * kPi * (1.0f - expf(-2.0f * kappa))));
+    }
+}
+
 // feats: the k_encode output for the same samples.
 __global__ void __launch_bounds__(kInferWarps * 32) k_infer(Model M, const float4* __restrict__ in, uint32_t n_host,
                                                             const uint32_t* __restrict__ n_dev,
@@ -502,7 +517,8 @@ spt_status Guide::alloc(spt_context* c, const spt_guide_config& cfg_) {
     if ((st = ensure_train_buffers(cfg.batch)) != SPT_OK) return st;
     const uint32_t n_cache = cache_res * cache_res * cache_res * 6;
     if ((st = ensure_features(n_cache)) != SPT_OK) return st;
-    SPT_CUDA(ctx, cudaMalloc(&cache, static_cast<size_t>(n_cache) * kOutUsed * sizeof(float)));
+    SPT_CUDA(ctx, cudaMalloc(&cache, static_cast<size_t>(n_cache) * kCacheEntry * sizeof(float)));
+    SPT_CUDA(ctx, cudaMalloc(&cache_raw, static_cast<size_t>(n_cache) * kOutUsed * sizeof(float)));
     SPT_CUDA(ctx, cudaMalloc(&cache_in, static_cast<size_t>(n_cache) * 3 * sizeof(float4)));
     return refresh();
 }
@@ -527,13 +543,13 @@ spt_status Guide::ensure_features(uint32_t n) {
 
 spt_status Guide::refresh_cache() {
     const uint32_t n = cache_res * cache_res * cache_res * 6;
-    if (!cache) {
-        SPT_CUDA(ctx, cudaMalloc(&cache, static_cast<size_t>(n) * kOutUsed * sizeof(float)));
-        SPT_CUDA(ctx, cudaMalloc(&cache_in, static_cast<size_t>(n) * 3 * sizeof(float4)));
-    }
     k_cache_inputs<<<256, 256, 0, ctx->stream>>>(model, cache_res, cache_in);
     SPT_CUDA(ctx, cudaGetLastError());
-    return infer(cache_in, n, cache, ctx->stream);
+    spt_status st = infer(cache_in, n, cache_raw, ctx->stream);
+    if (st != SPT_OK) return st;
+    k_cache_pack<<<256, 256, 0, ctx->stream>>>(cache_raw, n, cache);
+    SPT_CUDA(ctx, cudaGetLastError());
+    return SPT_OK;
 }
 
 spt_status Guide::infer(const float4* d_in, uint32_t n, float* d_out, cudaStream_t s) {

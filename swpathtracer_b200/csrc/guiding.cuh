@@ -275,5 +275,39 @@ __device__ __forceinline__ V3 mixture_sample(const Lobe (&lb)[kLobes], float u0,
     return normalize(t * (s * cosf(phi)) + b * (s * sinf(phi)) + n * w);
 }
 
+// ---- the lobe cache that guided rendering samples (Guide::refresh_cache) -----------------------
+// An entry holds the 8 lobes as {mu.xyz, kappa, w, w * C(kappa)} with C(kappa) = kappa / (2 pi
+// (1 - e^{-2 kappa})) the vMF normalisation, so the density of a direction costs one exp per lobe.
+constexpr int kCacheLobe = 6;
+constexpr int kCacheEntry = kLobes * kCacheLobe;   // 48 floats
+
+__device__ __forceinline__ float cached_mixture_pdf(const float* e, V3 w) {
+    float q = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kLobes; ++k) {
+        const float* l = e + kCacheLobe * k;
+        const float c = l[0] * w.x + l[1] * w.y + l[2] * w.z;
+        q += l[5] * expf(l[3] * (c - 1.0f));
+    }
+    return q;
+}
+
+// A direction from the cached mixture: the lobe by its weight, then Jakob's vMF sampler.
+__device__ __forceinline__ V3 cached_mixture_sample(const float* e, float u0, float u1, float u2) {
+    int k = 0;
+    float acc = e[4];
+    while (k < kLobes - 1 && u0 >= acc) acc += e[kCacheLobe * (++k) + 4];
+    const float* l = e + kCacheLobe * k;
+    const float kappa = l[3];
+    const float w = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * kappa)) / kappa;
+    const float s = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+    const float phi = 2.0f * kPi * u2;
+    const V3 n = v3(l[0], l[1], l[2]);
+    const V3 a = fabsf(n.x) > 0.9f ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
+    const V3 t = normalize(cross(a, n));
+    const V3 b = cross(n, t);
+    return normalize(t * (s * cosf(phi)) + b * (s * sinf(phi)) + n * w);
+}
+
 }  // namespace guide
 }  // namespace spt

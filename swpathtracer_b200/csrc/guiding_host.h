@@ -36,7 +36,8 @@ struct Guide {
     // rendering samples, refreshed after every round of training
     static constexpr uint32_t kCacheRes = 32;
     uint32_t cache_res = kCacheRes;
-    float* cache = nullptr;        // kCacheRes^3 * 6 * 40 floats
+    float* cache = nullptr;        // kCacheRes^3 * 6 entries of kCacheEntry floats
+    float* cache_raw = nullptr;    // the same entries as decoded lobes (40 floats), before packing
     float4* cache_in = nullptr;    // the network inputs of the cache entries
 
     spt_status alloc(spt_context* c, const spt_guide_config& cfg);
@@ -53,6 +54,7 @@ struct Guide {
     ~Guide() {
         if (feats) cudaFree(feats);
         if (cache) cudaFree(cache);
+        if (cache_raw) cudaFree(cache_raw);
         if (cache_in) cudaFree(cache_in);
         for (void* p : train_allocs) cudaFree(p);
         for (void* p : allocations) cudaFree(p);

@@ -68,7 +68,7 @@ struct Counters {
 struct GuideIO {
     float mix;
     uint32_t rec_cap;
-    const float* cache;    // the guide's mixture per (position cell, normal axis): 40 floats each
+    const float* cache;    // the guide's mixture per (position cell, normal axis): guide::kCacheEntry floats each
     uint32_t cache_res;    // cells per axis over the guide's box
     float lo[3], inv_ext[3];
     float4* rec;           // 4 float4 per record (spt_guide_record layout)
@@ -335,7 +335,8 @@ __global__ void __launch_bounds__(256) k_shade(Wave W, Counters* __restrict__ ct
                 float pdf;
                 const uint32_t gi = (GUIDED && guidable(J.S, m)) ? cache_cell(G, pos, nrm) : kNoRec;
                 if (GUIDED && gi != kNoRec) {
-                    const GuidedSample gs = guided_sample(J.S, m, frame, wo, G.cache + 40ull * gi, G.mix, bs);
+                    const GuidedSample gs =
+                        guided_sample(J.S, m, frame, wo, G.cache + static_cast<uint64_t>(guide::kCacheEntry) * gi, G.mix, bs);
                     f = gs.f;
                     refl = gs.refl;
                     wi = gs.wi_local;
