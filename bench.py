@@ -127,14 +127,15 @@ def cpu_baseline(packed, rays_np, budget_rays):
     return out
 
 
-def guided_vs_plain(spt, scenes, dev, torch, name, sb, spp, ref_spp, steps, seeds=(7, 8, 9, 10), mix=0.5):
+def guided_vs_plain(spt, scenes, dev, torch, name, sb, spp, ref_spp, steps, seeds=(7, 8, 9, 10), mix=0.5,
+                    cache_res=0):
     """Equal-time relMSE of guided vs plain path tracing (128^2, max length 5).  Plain and guided both
     render `spp` samples per seed; each image's relMSE mean((I - R)^2 / (R^2 + 1e-2)) against a
     `ref_spp` plain render is multiplied by its wall time (relMSE falls as 1/time), and the ratio
     plain / guided of the products, summed over the seeds, is the relMSE ratio at equal time
     (> 1: guiding wins).  The guided time includes the guide's online training (`steps` Adam steps of
     2^16 records) and its lobe-cache refreshes; each seed trains a fresh guide, which samples its
-    mixture with probability `mix`."""
+    mixture with probability `mix` from a lobe cache of `cache_res`^3 cells (0: the default)."""
     import numpy as np
     gs = spt.GpuScene(dev, sb.build())
     cam = scenes.box_camera(128, 128)
@@ -160,7 +161,8 @@ def guided_vs_plain(spt, scenes, dev, torch, name, sb, spp, ref_spp, steps, seed
     for seed in seeds:
         plain, t = render(spp, seed)
         ep, tp = ep + relmse(plain, ref), tp + t
-        g = spt.Guide(dev, spt.guide_config(batch=1 << 16, max_steps=steps, mix=mix, seed=seed))
+        g = spt.Guide(dev, spt.guide_config(batch=1 << 16, max_steps=steps, mix=mix, seed=seed,
+                                                 cache_res=cache_res))
         guided, t = render(spp, seed, g)
         eg, tg = eg + relmse(guided, ref), tg + t
         g.close()

@@ -280,6 +280,8 @@ typedef struct spt_guide_config {
     uint32_t max_steps;            /* optimiser steps per guided render before the model is frozen */
     float mix;                     /* probability of sampling the guiding distribution */
     uint64_t seed;                 /* parameter initialisation */
+    uint32_t cache_res;            /* cells per axis of the lobe cache guided renders sample: 4..64, 0 = 32 */
+    uint32_t reserved;             /* must be 0 */
 } spt_guide_config;
 
 /* One training record: a scattering event and the radiance it led to. */

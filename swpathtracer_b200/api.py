@@ -250,11 +250,12 @@ def autotune(device, jobs, cache_path=None):
     return t
 
 
-def guide_config(box_min=(0, 0, 0), box_max=(1, 1, 1), lr=1e-2, batch=1 << 18, max_steps=64, mix=0.5, seed=1):
+def guide_config(box_min=(0, 0, 0), box_max=(1, 1, 1), lr=1e-2, batch=1 << 18, max_steps=64, mix=0.5, seed=1,
+                 cache_res=0):
     c = abi.GuideConfig()
     for k in range(3):
         c.box_min[k], c.box_max[k] = box_min[k], box_max[k]
-    c.lr, c.batch, c.max_steps, c.mix, c.seed = lr, batch, max_steps, mix, seed
+    c.lr, c.batch, c.max_steps, c.mix, c.seed, c.cache_res = lr, batch, max_steps, mix, seed, cache_res
     return c
 
 

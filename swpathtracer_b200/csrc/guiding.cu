@@ -515,6 +515,7 @@ spt_status Guide::alloc(spt_context* c, const spt_guide_config& cfg_) {
     // everything a guided render needs is allocated here, so renders and training steps allocate
     // nothing: the training buffers of one batch, the lobe cache and its inference scratch
     if ((st = ensure_train_buffers(cfg.batch)) != SPT_OK) return st;
+    cache_res = cfg.cache_res ? cfg.cache_res : kCacheRes;
     const uint32_t n_cache = cache_res * cache_res * cache_res * 6;
     if ((st = ensure_features(n_cache)) != SPT_OK) return st;
     SPT_CUDA(ctx, cudaMalloc(&cache, static_cast<size_t>(n_cache) * kCacheEntry * sizeof(float)));

@@ -278,6 +278,10 @@ __device__ __forceinline__ V3 mixture_sample(const Lobe (&lb)[kLobes], float u0,
 // ---- the lobe cache that guided rendering samples (Guide::refresh_cache) -----------------------
 // An entry holds the 8 lobes as {mu.xyz, kappa, w, w * C(kappa)} with C(kappa) = kappa / (2 pi
 // (1 - e^{-2 kappa})) the vMF normalisation, so the density of a direction costs one exp per lobe.
+// Guided shading keeps the whole entry in registers: every index into it below is a compile-time
+// constant once the lobe loops unroll.  The mixture is a sampling density, not part of the
+// reference's exact ray arithmetic, so it uses the fast exp/log/sincos intrinsics and fused
+// multiply-adds; sampling and density use the same ones, so they stay consistent.
 constexpr int kCacheLobe = 6;
 constexpr int kCacheEntry = kLobes * kCacheLobe;   // 48 floats
 
@@ -286,27 +290,44 @@ __device__ __forceinline__ float cached_mixture_pdf(const float* e, V3 w) {
 #pragma unroll
     for (int k = 0; k < kLobes; ++k) {
         const float* l = e + kCacheLobe * k;
-        const float c = l[0] * w.x + l[1] * w.y + l[2] * w.z;
-        q += l[5] * expf(l[3] * (c - 1.0f));
+        const float c = __fmaf_rn(l[0], w.x, __fmaf_rn(l[1], w.y, __fmul_rn(l[2], w.z)));
+        q = __fmaf_rn(l[5], __expf(__fmul_rn(l[3], c - 1.0f)), q);
     }
     return q;
 }
 
-// A direction from the cached mixture: the lobe by its weight, then Jakob's vMF sampler.
+// A direction from the cached mixture: the first lobe whose cumulative weight exceeds u0 (the last
+// one if rounding leaves u0 above the sum), picked by selects over the unrolled lobes, then Jakob's
+// vMF sampler around its mean, in the orthonormal basis of Duff et al., "Building an Orthonormal
+// Basis, Revisited" (JCGT 2017).
 __device__ __forceinline__ V3 cached_mixture_sample(const float* e, float u0, float u1, float u2) {
-    int k = 0;
-    float acc = e[4];
-    while (k < kLobes - 1 && u0 >= acc) acc += e[kCacheLobe * (++k) + 4];
-    const float* l = e + kCacheLobe * k;
-    const float kappa = l[3];
-    const float w = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * kappa)) / kappa;
-    const float s = sqrtf(fmaxf(0.0f, 1.0f - w * w));
-    const float phi = 2.0f * kPi * u2;
-    const V3 n = v3(l[0], l[1], l[2]);
-    const V3 a = fabsf(n.x) > 0.9f ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
-    const V3 t = normalize(cross(a, n));
-    const V3 b = cross(n, t);
-    return normalize(t * (s * cosf(phi)) + b * (s * sinf(phi)) + n * w);
+    const float* last = e + kCacheLobe * (kLobes - 1);
+    float mx = last[0], my = last[1], mz = last[2], kappa = last[3];
+    float acc = 0.0f;
+    bool found = false;
+#pragma unroll
+    for (int k = 0; k < kLobes - 1; ++k) {
+        const float* l = e + kCacheLobe * k;
+        acc += l[4];
+        const bool take = !found && u0 < acc;
+        mx = take ? l[0] : mx;
+        my = take ? l[1] : my;
+        mz = take ? l[2] : mz;
+        kappa = take ? l[3] : kappa;
+        found = found || take;
+    }
+    const float w = __fmaf_rn(__logf(__fmaf_rn(1.0f - u1, __expf(-2.0f * kappa), u1)), __frcp_rn(kappa), 1.0f);
+    const float s = sqrtf(fmaxf(0.0f, __fmaf_rn(-w, w, 1.0f)));
+    float sn, cs;
+    __sincosf(2.0f * kPi * u2, &sn, &cs);
+    const float sg = copysignf(1.0f, mz);
+    const float a = -__frcp_rn(sg + mz), b = mx * my * a;
+    const V3 t = v3(__fmaf_rn(sg * mx * mx, a, 1.0f), sg * b, -sg * mx);
+    const V3 bt = v3(b, __fmaf_rn(my * my, a, sg), -my);
+    const float ts = s * cs, bs = s * sn;
+    const V3 r = v3(__fmaf_rn(t.x, ts, __fmaf_rn(bt.x, bs, mx * w)), __fmaf_rn(t.y, ts, __fmaf_rn(bt.y, bs, my * w)),
+                    __fmaf_rn(t.z, ts, __fmaf_rn(bt.z, bs, mz * w)));
+    return r * rsqrtf(__fmaf_rn(r.x, r.x, __fmaf_rn(r.y, r.y, r.z * r.z)));
 }
 
 }  // namespace guide

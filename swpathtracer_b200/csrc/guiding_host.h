@@ -34,9 +34,9 @@ struct Guide {
     uint32_t feats_cap = 0;
     // the mixture cached per (cell of a cache_res^3 grid over the box, normal axis): what guided
     // rendering samples, refreshed after every round of training
-    static constexpr uint32_t kCacheRes = 32;
+    static constexpr uint32_t kCacheRes = 32;   // cells per axis unless the config names another
     uint32_t cache_res = kCacheRes;
-    float* cache = nullptr;        // kCacheRes^3 * 6 entries of kCacheEntry floats
+    float* cache = nullptr;        // cache_res^3 * 6 entries of kCacheEntry floats
     float* cache_raw = nullptr;    // the same entries as decoded lobes (40 floats), before packing
     float4* cache_in = nullptr;    // the network inputs of the cache entries
 
