@@ -49,20 +49,10 @@ struct GuidedSample {
 __device__ __forceinline__ GuidedSample guided_sample(const DevScene& S, const DevMaterial& m, const float* frame,
                                                       V3 wo, const float* entry, float mix, Stream& s) {
     const DevBsdf b = S.bsdf[S.layer_ids[m.layer_begin]];
-    float e[guide::kCacheEntry];
-    const float4* src = reinterpret_cast<const float4*>(entry);
-#pragma unroll
-    for (int k = 0; k < guide::kCacheEntry / 4; ++k) {
-        const float4 v = __ldg(src + k);
-        e[4 * k] = v.x;
-        e[4 * k + 1] = v.y;
-        e[4 * k + 2] = v.z;
-        e[4 * k + 3] = v.w;
-    }
     GuidedSample g;
     if (s.next() < mix) {
         const float u0 = s.next(), u1 = s.next(), u2 = s.next();
-        g.wi_world = guide::cached_mixture_sample(e, u0, u1, u2);
+        g.wi_world = guide::cached_mixture_sample(entry, u0, u1, u2);
         g.wi_local = mat_tmul(frame, g.wi_world);
     } else {
         const BSample bs = bsdf_sample(b, wo, s);
@@ -72,7 +62,7 @@ __device__ __forceinline__ GuidedSample guided_sample(const DevScene& S, const D
     const V3 wi = g.wi_local;
     g.f = wi.y > 0.0f ? bsdf_f(b, wo, wi) : v3(0.0f, 0.0f, 0.0f);
     g.refl = wi.y > 0.0f ? bsdf_refl(b, wo, wi) : v3(0.0f, 0.0f, 0.0f);
-    g.p = mix * guide::cached_mixture_pdf(e, g.wi_world) + (1.0f - mix) * sampler_density(b, wo, wi);
+    g.p = mix * guide::cached_mixture_pdf(entry, g.wi_world) + (1.0f - mix) * sampler_density(b, wo, wi);
     return g;
 }
 

@@ -84,18 +84,20 @@ __global__ void k_cache_inputs(Model M, uint32_t R, float4* __restrict__ in) {
     }
 }
 
-// Decoded lobes {mu.xyz, kappa, w} -> cache entries {mu.xyz, kappa, w, w * C(kappa)} (guiding.cuh).
+// Decoded lobes {mu.xyz, kappa, w} -> field-major cache entries of mu.xyz, kappa, w, w * C(kappa)
+// (guiding.cuh).
 __global__ void k_cache_pack(const float* __restrict__ raw, uint32_t n, float* __restrict__ out) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n * kLobes; i += gridDim.x * blockDim.x) {
         const float* l = raw + 5ull * i;
-        float* o = out + static_cast<uint64_t>(kCacheLobe) * i;
+        const uint32_t lobe = i % kLobes;
+        float* o = out + static_cast<uint64_t>(kCacheEntry) * (i / kLobes) + lobe;
         const float kappa = l[3];
-        o[0] = l[0];
-        o[1] = l[1];
-        o[2] = l[2];
-        o[3] = kappa;
-        o[4] = l[4];
-        o[5] = l[4] * (kappa / (2.0f * kPi * (1.0f - expf(-2.0f * kappa))));
+        o[kLobes * kMuX] = l[0];
+        o[kLobes * kMuY] = l[1];
+        o[kLobes * kMuZ] = l[2];
+        o[kLobes * kKappa] = kappa;
+        o[kLobes * kWeight] = l[4];
+        o[kLobes * kWeightC] = l[4] * (kappa / (2.0f * kPi * (1.0f - expf(-2.0f * kappa))));
     }
 }
 

@@ -276,46 +276,55 @@ __device__ __forceinline__ V3 mixture_sample(const Lobe (&lb)[kLobes], float u0,
 }
 
 // ---- the lobe cache that guided rendering samples (Guide::refresh_cache) -----------------------
-// An entry holds the 8 lobes as {mu.xyz, kappa, w, w * C(kappa)} with C(kappa) = kappa / (2 pi
-// (1 - e^{-2 kappa})) the vMF normalisation, so the density of a direction costs one exp per lobe.
-// Guided shading keeps the whole entry in registers: every index into it below is a compile-time
-// constant once the lobe loops unroll.  The mixture is a sampling density, not part of the
-// reference's exact ray arithmetic, so it uses the fast exp/log/sincos intrinsics and fused
-// multiply-adds; sampling and density use the same ones, so they stay consistent.
-constexpr int kCacheLobe = 6;
+// An entry holds six fields of the 8 lobes, field-major: mu.x[8], mu.y[8], mu.z[8], kappa[8], w[8],
+// wc[8] with wc = w * C(kappa) and C(kappa) = kappa / (2 pi (1 - e^{-2 kappa})) the vMF
+// normalisation, so the density of a direction costs one exp per lobe.  Field-major, the density
+// streams one float4 of each field per four lobes, and sampling reads the weights and then only the
+// chosen lobe: guided shading never holds the whole entry in registers.  The mixture is a sampling
+// density, not part of the reference's exact ray arithmetic, so it uses the fast exp/log/sincos
+// intrinsics and fused multiply-adds; sampling and density use the same ones, so they agree.
+constexpr int kCacheLobe = 6;                      // fields per lobe
 constexpr int kCacheEntry = kLobes * kCacheLobe;   // 48 floats
+enum CacheField { kMuX = 0, kMuY = 1, kMuZ = 2, kKappa = 3, kWeight = 4, kWeightC = 5 };
 
-__device__ __forceinline__ float cached_mixture_pdf(const float* e, V3 w) {
+__device__ __forceinline__ float cached_mixture_pdf(const float* entry, V3 w) {
+    const float4* e = reinterpret_cast<const float4*>(entry);
     float q = 0.0f;
 #pragma unroll
-    for (int k = 0; k < kLobes; ++k) {
-        const float* l = e + kCacheLobe * k;
-        const float c = __fmaf_rn(l[0], w.x, __fmaf_rn(l[1], w.y, __fmul_rn(l[2], w.z)));
-        q = __fmaf_rn(l[5], __expf(__fmul_rn(l[3], c - 1.0f)), q);
+    for (int h = 0; h < 2; ++h) {
+        const float4 mx = __ldg(e + 2 * kMuX + h), my = __ldg(e + 2 * kMuY + h), mz = __ldg(e + 2 * kMuZ + h);
+        const float4 ka = __ldg(e + 2 * kKappa + h), wc = __ldg(e + 2 * kWeightC + h);
+        const float c0 = __fmaf_rn(mx.x, w.x, __fmaf_rn(my.x, w.y, __fmul_rn(mz.x, w.z)));
+        const float c1 = __fmaf_rn(mx.y, w.x, __fmaf_rn(my.y, w.y, __fmul_rn(mz.y, w.z)));
+        const float c2 = __fmaf_rn(mx.z, w.x, __fmaf_rn(my.z, w.y, __fmul_rn(mz.z, w.z)));
+        const float c3 = __fmaf_rn(mx.w, w.x, __fmaf_rn(my.w, w.y, __fmul_rn(mz.w, w.z)));
+        q = __fmaf_rn(wc.x, __expf(__fmul_rn(ka.x, c0 - 1.0f)), q);
+        q = __fmaf_rn(wc.y, __expf(__fmul_rn(ka.y, c1 - 1.0f)), q);
+        q = __fmaf_rn(wc.z, __expf(__fmul_rn(ka.z, c2 - 1.0f)), q);
+        q = __fmaf_rn(wc.w, __expf(__fmul_rn(ka.w, c3 - 1.0f)), q);
     }
     return q;
 }
 
 // A direction from the cached mixture: the first lobe whose cumulative weight exceeds u0 (the last
-// one if rounding leaves u0 above the sum), picked by selects over the unrolled lobes, then Jakob's
-// vMF sampler around its mean, in the orthonormal basis of Duff et al., "Building an Orthonormal
-// Basis, Revisited" (JCGT 2017).
-__device__ __forceinline__ V3 cached_mixture_sample(const float* e, float u0, float u1, float u2) {
-    const float* last = e + kCacheLobe * (kLobes - 1);
-    float mx = last[0], my = last[1], mz = last[2], kappa = last[3];
+// one if rounding leaves u0 above the sum), then Jakob's vMF sampler around its mean, in the
+// orthonormal basis of Duff et al., "Building an Orthonormal Basis, Revisited" (JCGT 2017).
+__device__ __forceinline__ V3 cached_mixture_sample(const float* entry, float u0, float u1, float u2) {
+    const float4* e4 = reinterpret_cast<const float4*>(entry);
+    const float4 wa = __ldg(e4 + 2 * kWeight), wb = __ldg(e4 + 2 * kWeight + 1);
+    const float w8[kLobes] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+    uint32_t k = kLobes - 1;
     float acc = 0.0f;
     bool found = false;
 #pragma unroll
-    for (int k = 0; k < kLobes - 1; ++k) {
-        const float* l = e + kCacheLobe * k;
-        acc += l[4];
+    for (int j = 0; j < kLobes - 1; ++j) {
+        acc += w8[j];
         const bool take = !found && u0 < acc;
-        mx = take ? l[0] : mx;
-        my = take ? l[1] : my;
-        mz = take ? l[2] : mz;
-        kappa = take ? l[3] : kappa;
+        k = take ? static_cast<uint32_t>(j) : k;
         found = found || take;
     }
+    const float mx = __ldg(entry + kLobes * kMuX + k), my = __ldg(entry + kLobes * kMuY + k);
+    const float mz = __ldg(entry + kLobes * kMuZ + k), kappa = __ldg(entry + kLobes * kKappa + k);
     const float w = __fmaf_rn(__logf(__fmaf_rn(1.0f - u1, __expf(-2.0f * kappa), u1)), __frcp_rn(kappa), 1.0f);
     const float s = sqrtf(fmaxf(0.0f, __fmaf_rn(-w, w, 1.0f)));
     float sn, cs;
