@@ -173,6 +173,53 @@ def guided_vs_plain(spt, scenes, dev, torch, name, sb, spp, ref_spp, steps, seed
             name + "_equal_time_relmse_ratio_plain_over_guided": round((ep * tp) / (eg * tg), 4)}
 
 
+def guided_batch_sample(spt, scenes, dev, torch, n=8, res_cap=256, spp=1024, ref_spp=16384, steps=32):
+    """Guided vs plain on the first `n` scenes of the 64-scene batch set (resolution capped at
+    `res_cap`^2, `spp` samples, max length 5): the same equal-time relMSE ratio as guided_vs_plain,
+    with (relMSE x wall time) summed over the scenes, each against a `ref_spp` plain render.  Each
+    scene trains a fresh guide (`steps` Adam steps of 2^16 records, mix 0.5) over the unit box."""
+    import numpy as np
+
+    def relmse(a, b):
+        return float(np.mean((a - b) ** 2 / (b ** 2 + 1e-2)))
+
+    ep = eg = 0.0
+    segs_p = segs_g = 0
+    per_scene = []
+    for i, (sb, cam0, _, _) in enumerate(scenes.batched_scenes()[:n]):
+        res = min(cam0.width, res_cap)
+        cam = scenes.box_camera(res, res)
+        gs = spt.GpuScene(dev, sb.build())
+        img = torch.empty(res * res * 3, dtype=torch.float32, device="cuda")
+
+        def render(k, seed, guide=None):
+            p = scenes.pt_params(spp=k, sampler="jittered", termination="max-length", path_length=5, seed=seed)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if guide is None:
+                st = gs.pathtrace_device(cam, p, img.data_ptr())
+            else:
+                st = gs.pathtrace_guided_device(cam, p, guide, img.data_ptr())
+            torch.cuda.synchronize()
+            return img.cpu().numpy().copy(), time.perf_counter() - t0, st.segments
+
+        render(16, 1)
+        ref, _, _ = render(ref_spp, 99)
+        plain, tp, sp = render(spp, 7 + i)
+        g = spt.Guide(dev, spt.guide_config(batch=1 << 16, max_steps=steps, mix=0.5, seed=7 + i))
+        guided, tg, sg = render(spp, 7 + i, g)
+        g.close()
+        gs.close()
+        a, b = relmse(plain, ref) * tp, relmse(guided, ref) * tg
+        ep, eg = ep + a, eg + b
+        segs_p, segs_g = segs_p + sp, segs_g + sg
+        per_scene.append(round(a / b, 3))
+    key = "guided_batch_first%d_%dpx_%dspp" % (n, res_cap, spp)
+    return {key + "_equal_time_relmse_ratio_plain_over_guided": round(ep / eg, 4),
+            key + "_per_scene_ratios": per_scene,
+            key + "_segments_guided_over_plain": round(segs_g / segs_p, 4)}
+
+
 def cpu_pathtrace_baseline(subdiv):
     """The reference's own PathTracer::render (oracle/_ref) on this host's cores, on bounded samples of
     the two path-tracing workloads (4 spp of the box scene, 1 spp of the layered 1.3M-tri scene).
@@ -401,6 +448,8 @@ def main():
                                       scenes.window_room_scene(0.1), 16384, 262144, 32))
         extras.update(guided_vs_plain(spt, scenes, dev, torch, "guided_small_light_128x128",
                                       scenes.small_light_box_scene(), 4096, 16384, 32, seeds=(7,)))
+        # guided rendering on a sample of the batch set (box with a 0.25 x 0.25 ceiling light)
+        extras.update(guided_batch_sample(spt, scenes, dev, torch))
         out["submetrics"] = extras
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(packed, rays_np, 1 << 22)
