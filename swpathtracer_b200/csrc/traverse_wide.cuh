@@ -181,7 +181,10 @@ struct WideTraversal {
     uint32_t g_base, g_hits, g_imask, t_base, t_mask;
     bool exact;
 
-    // Returns false when the ray is already finished (empty scene or root box missed).
+    // Returns false when the ray is already finished (empty scene or root box missed).  The root node
+    // itself is visited by the first step(): a lane that takes a new ray while the rest of its warp
+    // is mid-traversal then tests the root's children together with the other lanes' node visits,
+    // not alone in the refill branch.
     __device__ __forceinline__ bool start(const DevScene& S, V3 o_, V3 d_, bool exact_ = false) {
         o = o_;
         d = d_;
@@ -198,11 +201,18 @@ struct WideTraversal {
         if (!slab(ri, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], t0, t1))
             return false;
         r.o = o;
-        r.ix = safe_inv(d.x);
-        r.iy = safe_inv(d.y);
-        r.iz = safe_inv(d.z);
+        // safe_inv without dividing again: 1/d is already in ri unless |d| <= 1e-20
+        r.ix = fabsf(d.x) > 1e-20f ? ri.inv.x : copysignf(1.0f / 1e-20f, d.x);
+        r.iy = fabsf(d.y) > 1e-20f ? ri.inv.y : copysignf(1.0f / 1e-20f, d.y);
+        r.iz = fabsf(d.z) > 1e-20f ? ri.inv.z : copysignf(1.0f / 1e-20f, d.z);
         r.inv_oct = (r.ix >= 0.0f ? 0u : 1u) | (r.iy >= 0.0f ? 0u : 2u) | (r.iz >= 0.0f ? 0u : 4u);
-        wide_node_hits(S, r, 0, h.t, g_base, g_hits, g_imask, t_base, t_mask);
+        // a pending visit of node 0: one hit child (slot 0, whose near-to-far key is inv_oct) of a
+        // parent whose first child is node 0
+        g_base = 0;
+        g_imask = 1u;
+        g_hits = 1u << r.inv_oct;
+        t_base = 0;
+        t_mask = 0;
         return true;
     }
 
