@@ -190,6 +190,12 @@ const char* spt_last_error(const spt_context* ctx);
 /* Host build of the reference's full-sweep SAH tree, node for node
  * (acceleration/sbvh.cpp:12-37, 58-421); n_threads <= 0 uses all cores. */
 spt_status spt_bvh_build(const spt_scene_desc* desc, int n_threads, spt_bvh** out);
+/* Device build of a binary SAH-quality tree in the same layout (Morton order + parallel
+ * locally-ordered clustering + SAH leaf collapse), in milliseconds instead of the host build's
+ * seconds.  It replaces SBVH::build (acceleration/sbvh.cpp:12-37) where the reference's exact tree is
+ * not needed: closest hits are the same except the choice between primitives hit at an equal t, and
+ * hit counts are this tree's.  Deterministic for a given input. */
+spt_status spt_bvh_build_device(spt_context* ctx, const spt_scene_desc* desc, spt_bvh** out);
 spt_status spt_bvh_stats_get(const spt_bvh* bvh, spt_bvh_stats* out);   /* SBVH::getStatistics, sbvh.h:72 */
 /* Copies the flattened tree out; either array may be NULL to query sizes only. */
 spt_status spt_bvh_export(const spt_bvh* bvh, spt_bvh2_node* nodes, uint64_t* n_nodes,

@@ -74,12 +74,18 @@ class Device:
 
 
 class Bvh:
-    """The reference's SAH tree built on the host (acceleration/sbvh.cpp:12-37)."""
+    """A binary BVH for a packed scene.  By default the reference's own SAH tree, built on the host
+    (acceleration/sbvh.cpp:12-37).  With `device`, a tree of similar quality built on that device in
+    milliseconds (spt_bvh_build_device): the same closest hits except between primitives hit at an
+    equal t, and this tree's hit counts."""
 
-    def __init__(self, packed, n_threads=0):
+    def __init__(self, packed, n_threads=0, device=None):
         self.lib = native.lib()
         h = C.c_void_p()
-        native.check(self.lib.spt_bvh_build(packed.ref(), n_threads, C.byref(h)), None, "spt_bvh_build")
+        if device is None:
+            native.check(self.lib.spt_bvh_build(packed.ref(), n_threads, C.byref(h)), None, "spt_bvh_build")
+        else:
+            device.check(self.lib.spt_bvh_build_device(device.h, packed.ref(), C.byref(h)), "spt_bvh_build_device")
         self.h = h
 
     def close(self):

@@ -253,6 +253,24 @@ spt_status spt_bvh_build(const spt_scene_desc* desc, int n_threads, spt_bvh** ou
     return SPT_OK;
 }
 
+spt_status spt_bvh_build_device(spt_context* ctx, const spt_scene_desc* desc, spt_bvh** out) {
+    if (!ctx || !out) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    spt_status s = validate_desc(ctx, desc);
+    if (s != SPT_OK) return s;
+    SPT_CUDA(ctx, cudaSetDevice(ctx->device));
+    auto b = std::unique_ptr<spt_bvh>(new (std::nothrow) spt_bvh());
+    if (!b) return fail(ctx, SPT_ERR_OUT_OF_MEMORY, "host memory");
+    try {
+        s = build_ploc_tree(ctx, *desc, b->tree);
+    } catch (const std::bad_alloc&) {
+        return fail(ctx, SPT_ERR_OUT_OF_MEMORY, "host memory for the device BVH build");
+    }
+    if (s != SPT_OK) return s;
+    *out = b.release();
+    return SPT_OK;
+}
+
 spt_status spt_bvh_stats_get(const spt_bvh* bvh, spt_bvh_stats* out) {
     if (!bvh || !out) return SPT_ERR_INVALID_ARGUMENT;
     *out = bvh->tree.stats;

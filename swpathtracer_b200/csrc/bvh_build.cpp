@@ -204,8 +204,18 @@ bool build_sah_tree(const spt_scene_desc& d, int n_threads, HostBvh& out, const 
     }
     out.refs.resize(n);
     for (uint32_t i = 0; i < n; ++i) out.refs[i] = B.refs[i].id;
+    tree_statistics(out);
+    out.stats.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return true;
+}
+
+void tree_statistics(HostBvh& out) {
     // statistics as SBVH::collectTreeStatistics reports them (sbvh.cpp:517-575)
     spt_bvh_stats& s = out.stats;
+    const double build_ms = s.build_ms;
+    std::memset(&s, 0, sizeof(s));
+    s.build_ms = build_ms;
+    if (out.nodes.empty()) return;
     s.min_prims_leaf = std::numeric_limits<uint64_t>::max();
     std::vector<uint32_t> level{0}, nextl;
     uint64_t levels = 0;
@@ -230,8 +240,6 @@ bool build_sah_tree(const spt_scene_desc& d, int n_threads, HostBvh& out, const 
     }
     s.tree_height = levels ? levels - 1 : 0;
     s.num_unreferenced = 0;  // every primitive lands in exactly one leaf of an object-split tree
-    s.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    return true;
 }
 
 }  // namespace spt

@@ -28,6 +28,9 @@ struct HostBvh {
 // the result does not depend on the thread count.  Returns false on an input it cannot build.
 bool build_sah_tree(const spt_scene_desc& desc, int n_threads, HostBvh& out, const char** err);
 
+// Fills out.stats (all but build_ms) from out.nodes, as SBVH::collectTreeStatistics counts them.
+void tree_statistics(HostBvh& out);
+
 // Primitive bounds and centroid exactly as the reference computes them
 // (primitives/triangle.cpp:76-87, primitives/sphere.cpp:48-60).
 void prim_bounds(const spt_scene_desc& desc, uint32_t i, HostBox& box, float centroid[3]);

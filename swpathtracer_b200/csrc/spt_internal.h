@@ -52,6 +52,8 @@ namespace spt {
 
 // Status helpers: every entry point records a message and returns a status, never throws.
 spt_status fail(spt_context* ctx, spt_status s, const std::string& msg);
+// The device builder behind spt_bvh_build_device (bvh_gpu.cu).
+spt_status build_ploc_tree(spt_context* ctx, const spt_scene_desc& d, HostBvh& out);
 spt_status cuda_fail(spt_context* ctx, cudaError_t e, const char* what);
 #define SPT_CUDA(ctx, call)                                          \
     do {                                                             \

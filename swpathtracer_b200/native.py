@@ -19,6 +19,7 @@ PROTOTYPES = {
     "spt_destroy": (i32, [vp]),
     "spt_last_error": (C.c_char_p, [vp]),
     "spt_bvh_build": (i32, [vp, i32, C.POINTER(vp)]),
+    "spt_bvh_build_device": (i32, [vp, vp, C.POINTER(vp)]),
     "spt_bvh_stats_get": (i32, [vp, vp]),
     "spt_bvh_export": (i32, [vp, vp, vp, vp, vp]),
     "spt_bvh_free": (i32, [vp]),
