@@ -408,6 +408,25 @@ def main():
             e1.record()
             torch.cuda.synchronize()
             extras["primary_1920x1080_" + name + "_Mrays_s"] = round(1920 * 1080 * 10 / (e0.elapsed_time(e1) / 1e3) / 1e6, 2)
+        # the device-built tree (spt_bvh_build_device) of the same mesh: build time, and the headline
+        # queries over it (same closest hits except equal-t ties)
+        spt.Bvh(packed, device=dev).close()   # first call: module loading
+        t_dev = time.perf_counter()
+        dbvh = spt.Bvh(packed, device=dev)
+        extras["bvh_build_device_ms"] = round((time.perf_counter() - t_dev) * 1e3, 1)
+        dgs = spt.GpuScene(dev, packed, dbvh)
+        for _ in range(3):
+            dgs.intersect_device(d_rays.data_ptr(), n, d_hits.data_ptr(), 0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(20):
+            dgs.intersect_device(d_rays.data_ptr(), n, d_hits.data_ptr(), 0)
+        e1.record()
+        torch.cuda.synchronize()
+        extras["device_tree_closest_hit_Mrays_s"] = round(n * 20 / (e0.elapsed_time(e1) / 1e3) / 1e6, 1)
+        dgs.close()
+        dbvh.close()
         # path tracing: the CPU-runnable box scene (20,492 tris, 256x256, 16 spp, max length 5) and the
         # 1.3M-tri layered scene (800x600, russian roulette after 3, max depth 16), Mpaths/s
         for key, sb, cam, prm in (

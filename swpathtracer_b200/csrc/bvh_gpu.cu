@@ -11,7 +11,7 @@
 //     Clustering for Bounding Volume Hierarchy Construction", IEEE TVCG 2018): every cluster finds
 //     the cluster within kRadius positions of it in Morton order whose union box has the smallest
 //     surface area; mutual nearest neighbours merge; the array is compacted; repeat until one is left;
-//  4. on the host, a bottom-up SAH pass with the reference's constants (a node costs 2 x 1.2 plus its
+//  4. a bottom-up SAH pass with the reference's constants (a node costs 2 x 1.2 plus its
 //     children's costs weighted by area ratio; a leaf costs 1 per primitive) turns each subtree that
 //     is cheaper as one leaf into a leaf of at most kMaxLeaf primitives;
 //  5. the depth-first, left-first layout and box rule of the reference's tree: the root box is the
@@ -37,7 +37,11 @@ namespace {
 
 constexpr int kRadius = 16;        // PLOC search radius (positions on each side)
 constexpr int kTile = 256;         // clusters per block of the neighbour search
-constexpr uint32_t kMaxLeaf = 8;   // primitives per collapsed leaf
+// Primitives per collapsed leaf.  The 8-wide collapse packs up to three per child slot anyway, and
+// on the 1.31M-triangle mesh small leaves traverse fastest: 2,584 Mrays/s at 1, 2,528 at 2, 2,463 at
+// 3, 2,259 at 8 (the reference's own tree: 2,689).  At 1 the tree has twice the nodes, and the host
+// side of scene creation (the 8-wide collapse) takes 1.06 s instead of 0.58 s.
+constexpr uint32_t kMaxLeaf = 2;
 
 // glm::min / glm::max as the reference uses them (aabb.h)
 __device__ __forceinline__ float gmin_d(float x, float y) { return (y < x) ? y : x; }
@@ -141,13 +145,28 @@ struct Nodes {
     int2* child;
 };
 
+// Per-node state of the collapse (bottom-up) and of the depth-first layout (top-down).
+struct Tree {
+    uint32_t* cnt;       // primitives below
+    float* cost;         // SAH cost of the subtree as emitted
+    uint8_t* col;        // emitted as one leaf
+    uint32_t* outsize;   // output nodes the subtree emits
+    uint32_t* idx;       // output index (emitted nodes)
+    uint32_t* rb;        // offset of the subtree's first primitive in the reference list
+    uint8_t* state;      // 1: emitted inner node, 2: emitted leaf, 0: inside an emitted leaf
+};
+
 __global__ void k_leaves(const uint32_t* __restrict__ order, uint32_t n, const float4* __restrict__ bmin,
-                         const float4* __restrict__ bmax, Nodes N, uint32_t* __restrict__ cur) {
+                         const float4* __restrict__ bmax, Nodes N, Tree T, uint32_t* __restrict__ cur) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t p = order[i];
         N.mn[i] = bmin[p];
         N.mx[i] = bmax[p];
         N.child[i] = make_int2(-1, static_cast<int>(p));
+        T.cnt[i] = 1u;
+        T.cost[i] = 1.0f;
+        T.col[i] = 1u;
+        T.outsize[i] = 1u;
         cur[i] = i;
     }
 }
@@ -233,6 +252,83 @@ __global__ void k_compact(const uint32_t* __restrict__ next, const uint32_t* __r
     }
 }
 
+// The nodes one clustering pass made, whose children all come from earlier passes: primitive count,
+// SAH cost with the reference's constants (a node 2 x 1.2 plus its children's costs weighted by area
+// ratio, a leaf 1 per primitive), and whether the subtree is emitted as one leaf (at most kMaxLeaf
+// primitives, and no costlier than splitting).
+__global__ void k_up(Nodes N, Tree T, uint32_t a, uint32_t b) {
+    for (uint32_t v = a + blockIdx.x * blockDim.x + threadIdx.x; v < b; v += gridDim.x * blockDim.x) {
+        const int2 c = N.child[v];
+        const uint32_t l = static_cast<uint32_t>(c.x), r = static_cast<uint32_t>(c.y);
+        const uint32_t cnt = T.cnt[l] + T.cnt[r];
+        const float av = area_d(N.mn[v], N.mx[v]);
+        const float al = area_d(N.mn[l], N.mx[l]), ar = area_d(N.mn[r], N.mx[r]);
+        const float split = av > 0.0f ? 2.0f * 1.2f + (al / av) * T.cost[l] + (ar / av) * T.cost[r]
+                                      : 2.0f * 1.2f + T.cost[l] + T.cost[r];
+        const float leaf = static_cast<float>(cnt);
+        const bool col = cnt <= kMaxLeaf && leaf <= split;
+        T.cnt[v] = cnt;
+        T.cost[v] = col ? leaf : split;
+        T.col[v] = col ? 1u : 0u;
+        T.outsize[v] = col ? 1u : 1u + T.outsize[l] + T.outsize[r];
+    }
+}
+
+__global__ void k_root(Tree T, const uint32_t* __restrict__ cur) {
+    const uint32_t r = cur[0];
+    T.idx[r] = 0u;
+    T.rb[r] = 0u;
+    T.state[r] = T.col[r] ? 2u : 1u;
+}
+
+// One output node in the reference's layout; every box but the root's is inflated by 1e-3.
+__device__ __forceinline__ void write_node(spt_bvh2_node* out, uint32_t i, float4 mn, float4 mx, uint32_t right,
+                                           uint32_t count) {
+    float4* o = reinterpret_cast<float4*>(out + i);
+    if (i == 0) {
+        o[0] = make_float4(mn.x, mn.y, mn.z, __uint_as_float(right));
+        o[1] = make_float4(mx.x, mx.y, mx.z, __uint_as_float(count));
+    } else {
+        o[0] = make_float4(mn.x - 1e-3f, mn.y - 1e-3f, mn.z - 1e-3f, __uint_as_float(right));
+        o[1] = make_float4(mx.x + 1e-3f, mx.y + 1e-3f, mx.z + 1e-3f, __uint_as_float(count));
+    }
+}
+
+// The nodes of one pass, after every later pass (their parents): hand the children their output
+// index (left right after the parent, right after the left subtree) and reference offset, and write
+// the emitted nodes.
+__global__ void k_down(Nodes N, Tree T, uint32_t a, uint32_t b, spt_bvh2_node* __restrict__ out) {
+    for (uint32_t v = a + blockIdx.x * blockDim.x + threadIdx.x; v < b; v += gridDim.x * blockDim.x) {
+        const int2 c = N.child[v];
+        const uint32_t l = static_cast<uint32_t>(c.x), r = static_cast<uint32_t>(c.y);
+        const uint8_t st = T.state[v];
+        const uint32_t r0 = T.rb[v];
+        T.rb[l] = r0;
+        T.rb[r] = r0 + T.cnt[l];
+        if (st == 1u) {
+            const uint32_t i0 = T.idx[v];
+            const uint32_t ir = i0 + 1u + T.outsize[l];
+            T.idx[l] = i0 + 1u;
+            T.idx[r] = ir;
+            T.state[l] = T.col[l] ? 2u : 1u;
+            T.state[r] = T.col[r] ? 2u : 1u;
+            write_node(out, i0, N.mn[v], N.mx[v], ir, 0u);
+        } else {
+            T.state[l] = 0u;
+            T.state[r] = 0u;
+            if (st == 2u) write_node(out, T.idx[v], N.mn[v], N.mx[v], r0, T.cnt[v]);
+        }
+    }
+}
+
+__global__ void k_down_leaves(Nodes N, Tree T, uint32_t n, uint32_t* __restrict__ refs,
+                              spt_bvh2_node* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        refs[T.rb[i]] = static_cast<uint32_t>(N.child[i].y);
+        if (T.state[i] == 2u) write_node(out, T.idx[i], N.mn[i], N.mx[i], T.rb[i], 1u);
+    }
+}
+
 // Device buffers of one build, freed on every exit path.
 struct Scratch {
     std::vector<void*> ptrs;
@@ -248,11 +344,6 @@ struct Scratch {
         return e;
     }
 };
-
-float area_h(const float mn[3], const float mx[3]) {
-    const float l = mx[0] - mn[0], m = mx[1] - mn[1], n = mx[2] - mn[2];
-    return 2.0f * (l * (m + n) + m * n);
-}
 
 }  // namespace
 
@@ -293,6 +384,14 @@ spt_status build_ploc_tree(spt_context* ctx, const spt_scene_desc& d, HostBvh& o
     SPT_CUDA(ctx, S.get(&N.mn, n_nodes));
     SPT_CUDA(ctx, S.get(&N.mx, n_nodes));
     SPT_CUDA(ctx, S.get(&N.child, n_nodes));
+    Tree T;
+    SPT_CUDA(ctx, S.get(&T.cnt, n_nodes));
+    SPT_CUDA(ctx, S.get(&T.cost, n_nodes));
+    SPT_CUDA(ctx, S.get(&T.col, n_nodes));
+    SPT_CUDA(ctx, S.get(&T.outsize, n_nodes));
+    SPT_CUDA(ctx, S.get(&T.idx, n_nodes));
+    SPT_CUDA(ctx, S.get(&T.rb, n_nodes));
+    SPT_CUDA(ctx, S.get(&T.state, n_nodes));
     // sort and scan scratch, sized for the largest call
     size_t sort_bytes = 0, scan_bytes = 0;
     SPT_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, keys, keys2, vals, vals2,
@@ -312,7 +411,7 @@ spt_status build_ploc_tree(spt_context* ctx, const spt_scene_desc& d, HostBvh& o
     k_morton<<<grid, 256, 0, s>>>(cen, n, cb, keys, vals);
     size_t tb = std::max(sort_bytes, scan_bytes);
     SPT_CUDA(ctx, cub::DeviceRadixSort::SortPairs(temp, tb, keys, keys2, vals, vals2, static_cast<int>(n), 0, 63, s));
-    k_leaves<<<grid, 256, 0, s>>>(vals2, n, bmin, bmax, N, cur);
+    k_leaves<<<grid, 256, 0, s>>>(vals2, n, bmin, bmax, N, T, cur);
     SPT_CUDA(ctx, cudaGetLastError());
     SPT_CUDA(ctx, cudaMemcpyAsync(counters, &n, sizeof(n), cudaMemcpyHostToDevice, s));  // next free node
 
@@ -320,11 +419,12 @@ spt_status build_ploc_tree(spt_context* ctx, const spt_scene_desc& d, HostBvh& o
     uint32_t m = n;
     uint32_t passes = 0;
     uint32_t* h_count;
-    SPT_CUDA(ctx, cudaMallocHost(&h_count, sizeof(uint32_t)));
+    SPT_CUDA(ctx, cudaMallocHost(&h_count, 2 * sizeof(uint32_t)));
     struct PinnedFree {
         uint32_t* p;
         ~PinnedFree() { cudaFreeHost(p); }
     } pin{h_count};
+    std::vector<uint32_t> bounds{n};   // node ids created by pass p: [bounds[p], bounds[p + 1])
     while (m > 1) {
         if (++passes > n) return fail(ctx, SPT_ERR_INTERNAL, "device BVH build did not converge");
         const unsigned gm = static_cast<unsigned>(std::min<uint64_t>((m + 255) / 256, 8ull * sms));
@@ -334,98 +434,43 @@ spt_status build_ploc_tree(spt_context* ctx, const spt_scene_desc& d, HostBvh& o
         SPT_CUDA(ctx, cub::DeviceScan::ExclusiveSum(temp, tb, keep, pos, static_cast<int>(m), s));
         k_compact<<<gm, 256, 0, s>>>(next, keep, pos, m, cur2, counters + 1);
         SPT_CUDA(ctx, cudaGetLastError());
-        SPT_CUDA(ctx, cudaMemcpyAsync(h_count, counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        SPT_CUDA(ctx, cudaMemcpyAsync(h_count, counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         SPT_CUDA(ctx, cudaStreamSynchronize(s));
-        if (*h_count >= m) return fail(ctx, SPT_ERR_INTERNAL, "device BVH build made no progress");
-        m = *h_count;
+        if (h_count[1] >= m) return fail(ctx, SPT_ERR_INTERNAL, "device BVH build made no progress");
+        m = h_count[1];
+        bounds.push_back(h_count[0]);
         std::swap(cur, cur2);
     }
+    // bottom-up over the passes in creation order (children before parents): counts, SAH costs,
+    // collapse flags, emitted sizes; then top-down in reverse: output indices, reference offsets,
+    // output nodes and the reference list
     uint32_t root = 0;
     SPT_CUDA(ctx, cudaMemcpyAsync(&root, cur, sizeof(root), cudaMemcpyDeviceToHost, s));
-    std::vector<float4> hmn(n_nodes), hmx(n_nodes);
-    std::vector<int2> hch(n_nodes);
-    SPT_CUDA(ctx, cudaMemcpyAsync(hmn.data(), N.mn, n_nodes * sizeof(float4), cudaMemcpyDeviceToHost, s));
-    SPT_CUDA(ctx, cudaMemcpyAsync(hmx.data(), N.mx, n_nodes * sizeof(float4), cudaMemcpyDeviceToHost, s));
-    SPT_CUDA(ctx, cudaMemcpyAsync(hch.data(), N.child, n_nodes * sizeof(int2), cudaMemcpyDeviceToHost, s));
+    for (size_t p = 0; p + 1 < bounds.size(); ++p) {
+        const uint32_t a = bounds[p], b = bounds[p + 1];
+        k_up<<<static_cast<unsigned>(std::min<uint64_t>((b - a + 255) / 256, 8ull * sms)), 256, 0, s>>>(N, T, a, b);
+    }
+    k_root<<<1, 1, 0, s>>>(T, cur);
+    uint32_t n_out = 0;
+    SPT_CUDA(ctx, cudaMemcpyAsync(&n_out, T.outsize + root, sizeof(n_out), cudaMemcpyDeviceToHost, s));
     SPT_CUDA(ctx, cudaStreamSynchronize(s));
-
-    // bottom-up: primitive counts and SAH costs; collapse[v] marks subtrees emitted as one leaf
-    std::vector<uint32_t> cnt(n_nodes, 1);
-    std::vector<float> cost(n_nodes, 1.0f);
-    std::vector<uint8_t> collapse(n_nodes, 1);
-    {
-        std::vector<uint32_t> st{root}, post;
-        post.reserve(n_nodes);
-        while (!st.empty()) {   // children before parents: reverse of a pre-order with right pushed last
-            const uint32_t v = st.back();
-            st.pop_back();
-            post.push_back(v);
-            if (hch[v].x >= 0) {
-                st.push_back(static_cast<uint32_t>(hch[v].x));
-                st.push_back(static_cast<uint32_t>(hch[v].y));
-            }
-        }
-        for (size_t k = post.size(); k-- > 0;) {
-            const uint32_t v = post[k];
-            if (hch[v].x < 0) continue;
-            const uint32_t a = static_cast<uint32_t>(hch[v].x), b = static_cast<uint32_t>(hch[v].y);
-            cnt[v] = cnt[a] + cnt[b];
-            const float mn[3] = {hmn[v].x, hmn[v].y, hmn[v].z}, mx[3] = {hmx[v].x, hmx[v].y, hmx[v].z};
-            const float amn[3] = {hmn[a].x, hmn[a].y, hmn[a].z}, amx[3] = {hmx[a].x, hmx[a].y, hmx[a].z};
-            const float bmn_[3] = {hmn[b].x, hmn[b].y, hmn[b].z}, bmx_[3] = {hmx[b].x, hmx[b].y, hmx[b].z};
-            const float av = area_h(mn, mx);
-            const float split = av > 0.0f ? 2.0f * 1.2f + (area_h(amn, amx) / av) * cost[a] + (area_h(bmn_, bmx_) / av) * cost[b]
-                                          : 2.0f * 1.2f + cost[a] + cost[b];
-            const float leaf = static_cast<float>(cnt[v]);
-            collapse[v] = (cnt[v] <= kMaxLeaf && leaf <= split) ? 1 : 0;
-            cost[v] = collapse[v] ? leaf : split;
-        }
+    if (n_out == 0 || n_out > n_nodes) return fail(ctx, SPT_ERR_INTERNAL, "device BVH build: bad node count");
+    spt_bvh2_node* d_out;
+    uint32_t* d_refs;
+    SPT_CUDA(ctx, S.get(&d_out, n_out));
+    SPT_CUDA(ctx, S.get(&d_refs, n));
+    for (size_t p = bounds.size() - 1; p-- > 0;) {
+        const uint32_t a = bounds[p], b = bounds[p + 1];
+        k_down<<<static_cast<unsigned>(std::min<uint64_t>((b - a + 255) / 256, 8ull * sms)), 256, 0, s>>>(N, T, a, b,
+                                                                                                         d_out);
     }
-    // depth-first, left-first flatten with the reference's box rule
-    out.nodes.reserve(n_nodes);
-    out.refs.reserve(n);
-    struct Item {
-        uint32_t v;
-        int64_t parent;   // output index whose .right this node's index fills (-1: none)
-    };
-    std::vector<Item> st{{root, -1}};
-    std::vector<uint32_t> sub;
-    while (!st.empty()) {
-        const Item it = st.back();
-        st.pop_back();
-        const uint32_t idx = static_cast<uint32_t>(out.nodes.size());
-        if (it.parent >= 0) out.nodes[static_cast<size_t>(it.parent)].right = idx;
-        spt_bvh2_node o{};
-        const float4 a = hmn[it.v], b = hmx[it.v];
-        const float inf = idx == 0 ? 0.0f : 1e-3f;
-        o.min[0] = idx == 0 ? a.x : a.x - inf;
-        o.min[1] = idx == 0 ? a.y : a.y - inf;
-        o.min[2] = idx == 0 ? a.z : a.z - inf;
-        o.max[0] = idx == 0 ? b.x : b.x + inf;
-        o.max[1] = idx == 0 ? b.y : b.y + inf;
-        o.max[2] = idx == 0 ? b.z : b.z + inf;
-        if (collapse[it.v]) {
-            o.right = static_cast<uint32_t>(out.refs.size());
-            o.count = cnt[it.v];
-            sub.assign(1, it.v);   // the subtree's primitives, left to right
-            while (!sub.empty()) {
-                const uint32_t u = sub.back();
-                sub.pop_back();
-                if (hch[u].x < 0) {
-                    out.refs.push_back(static_cast<uint32_t>(hch[u].y));
-                } else {
-                    sub.push_back(static_cast<uint32_t>(hch[u].y));
-                    sub.push_back(static_cast<uint32_t>(hch[u].x));
-                }
-            }
-            out.nodes.push_back(o);
-        } else {
-            o.count = 0;
-            out.nodes.push_back(o);
-            st.push_back(Item{static_cast<uint32_t>(hch[it.v].y), static_cast<int64_t>(idx)});   // right, filled later
-            st.push_back(Item{static_cast<uint32_t>(hch[it.v].x), -1});                          // left = idx + 1
-        }
-    }
+    k_down_leaves<<<grid, 256, 0, s>>>(N, T, n, d_refs, d_out);
+    SPT_CUDA(ctx, cudaGetLastError());
+    out.nodes.resize(n_out);
+    out.refs.resize(n);
+    SPT_CUDA(ctx, cudaMemcpyAsync(out.nodes.data(), d_out, n_out * sizeof(spt_bvh2_node), cudaMemcpyDeviceToHost, s));
+    SPT_CUDA(ctx, cudaMemcpyAsync(out.refs.data(), d_refs, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    SPT_CUDA(ctx, cudaStreamSynchronize(s));
     if (out.refs.size() != n) return fail(ctx, SPT_ERR_INTERNAL, "device BVH build lost primitives");
     tree_statistics(out);
     out.stats.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
