@@ -439,8 +439,10 @@ def main():
             img = torch.empty(cam.width * cam.height * 3, dtype=torch.float32, device="cuda")
             for _ in range(2):
                 pgs.pathtrace_device(cam, prm, img.data_ptr())
-            runs = [pgs.pathtrace_device(cam, prm, img.data_ptr()) for _ in range(3)]
-            paths, segs, ms = (sum(r.paths for r in runs), sum(r.segments for r in runs), sum(r.gpu_ms for r in runs))
+            # seven renders of a few ms each; the median is robust to a transient on a shared machine
+            runs = sorted((pgs.pathtrace_device(cam, prm, img.data_ptr()) for _ in range(7)), key=lambda r: r.gpu_ms)
+            mid = runs[len(runs) // 2]
+            paths, segs, ms = mid.paths, mid.segments, mid.gpu_ms
             extras[key + "_Mpaths_s"] = round(paths / (ms / 1e3) / 1e6, 3)
             extras[key + "_Mrays_s"] = round(segs / (ms / 1e3) / 1e6, 2)
             extras[key + "_segments_per_path"] = round(segs / paths, 3)
