@@ -311,7 +311,10 @@ __global__ void __launch_bounds__(256, 3) k_shade(Wave W, Counters* __restrict__
         uint4 rr = make_uint4(kNoRec, kNoRec, kNoRec, kNoRec);
         if (j < n) {
             const uint32_t i = order ? order[j] : j;   // the slot this lane shades
-            const float4 o4 = cur.o[i], d4 = cur.d[i], b4 = cur.b[i], l4 = cur.l[i], h4 = hits[i];
+            // the slot's last use in this iteration (the buffer is rewritten as the next one's output):
+            // evict-first loads leave L2 to the scene
+            const float4 o4 = __ldcs(cur.o + i), d4 = __ldcs(cur.d + i), b4 = __ldcs(cur.b + i), l4 = __ldcs(cur.l + i),
+                         h4 = __ldcs(hits + i);
             if (GUIDED) rr = cur.r[i];
             const uint32_t pix = __float_as_uint(o4.w), sg = __float_as_uint(d4.w);
             const uint32_t jd = __float_as_uint(b4.w);

@@ -17,24 +17,22 @@ namespace {
 constexpr int kBlock = 128;
 
 // Persistent variant: wide traversal, lanes refilled from a global ray counter (traverse_wide.cuh).
-// 10 blocks of 128 per SM (at most 48 registers): 40 resident warps to hide the node-fetch latency
+// 10 blocks of 128 per SM (at most 48 registers): 40 resident warps to hide the node-fetch latency.
+// Rays are read and hits written once, with the evict-first (streaming) cache hint, so the ray and
+// hit streams (48 B per ray, 768 MB per 2^24 rays) push less of the scene out of L2: +1 %.
 __global__ void __launch_bounds__(kBlock, 10) k_intersect_df(DevScene S, const float4* __restrict__ rays, uint64_t n,
                                                          spt_hit* __restrict__ hits, uint32_t* status,
                                                          unsigned long long* next) {
     persistent_trace(
         S, n, next, status,
         [&](uint64_t i, V3& o, V3& d) {
-            const float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+            const float4 a = __ldcs(rays + 2 * i), b = __ldcs(rays + 2 * i + 1);
             o = f3v(a);
             d = f3v(b);
         },
         [&](uint64_t i, const Hit1& h) {
-            spt_hit out;
-            out.t = h.t;
-            out.prim_id = h.found ? slot_prim(S, h.slot) : SPT_MISS;
-            out.u = h.u;
-            out.v = h.v;
-            hits[i] = out;
+            __stcs(reinterpret_cast<float4*>(hits + i),
+                   make_float4(h.t, __uint_as_float(h.found ? slot_prim(S, h.slot) : SPT_MISS), h.u, h.v));
         });
 }
 
