@@ -450,7 +450,16 @@ def main():
         # batched uneven scenes: 64 seeded scenes (1k-500k tris, 128^2-1024^2, 64 spp) in one wavefront,
         # settings from the autotuner (its trials are not timed)
         batch = scenes.batched_scenes()
-        jobs = [(spt.GpuScene(dev, sb.build()), cam, prm) for sb, cam, prm, _ in batch]
+        packs = [sb.build() for sb, _, _, _ in batch]
+        # scene set-up of the 64 scenes (tree + device upload): the reference's tree built on the host,
+        # and the device-built tree (spt_bvh_build_device)
+        t_setup = time.perf_counter()
+        for p_ in packs:
+            spt.GpuScene(dev, p_, spt.Bvh(p_, device=dev)).close()
+        extras["batch64_setup_device_tree_s"] = round(time.perf_counter() - t_setup, 3)
+        t_setup = time.perf_counter()
+        jobs = [(spt.GpuScene(dev, p_), cam, prm) for p_, (_, cam, prm, _) in zip(packs, batch)]
+        extras["batch64_setup_host_tree_s"] = round(time.perf_counter() - t_setup, 3)
         bufs = [torch.empty(cam.width * cam.height * 3, dtype=torch.float32, device="cuda") for _, cam, _ in jobs]
         tune = spt.autotune(dev, jobs, None)
         st = spt.render_batch(dev, jobs, [b.data_ptr() for b in bufs], tune=tune)

@@ -164,21 +164,38 @@ spt_status validate_desc(spt_context* ctx, const spt_scene_desc* d) {
     return SPT_OK;
 }
 
-template <typename T>
-spt_status upload(spt_scene* sc, const std::vector<T>& host, const T** dst) {
-    if (host.empty()) {
+// Scene arrays placed in one device allocation at 256-byte aligned offsets, then copied in.
+struct Upload {
+    struct Entry {
+        const void* src;
+        size_t bytes, offset;
+        const void** dst;
+    };
+    std::vector<Entry> entries;
+    size_t total = 0;
+    template <typename T>
+    void add(const std::vector<T>& host, const T** dst) {
         *dst = nullptr;
+        if (host.empty()) return;
+        const size_t off = (total + 255) & ~static_cast<size_t>(255);
+        entries.push_back(Entry{host.data(), host.size() * sizeof(T), off, reinterpret_cast<const void**>(dst)});
+        total = off + host.size() * sizeof(T);
+    }
+    spt_status commit(spt_scene* sc) {
+        if (total == 0) return SPT_OK;
+        void* base = nullptr;
+        SPT_CUDA(sc->ctx, cudaMalloc(&base, total));
+        sc->allocations.push_back(base);
+        sc->bytes += total;
+        for (const Entry& e : entries) {
+            char* p = static_cast<char*>(base) + e.offset;
+            SPT_CUDA(sc->ctx, cudaMemcpy(p, e.src, e.bytes, cudaMemcpyHostToDevice));
+            *e.dst = p;
+        }
         return SPT_OK;
     }
-    void* p = nullptr;
-    size_t bytes = host.size() * sizeof(T);
-    SPT_CUDA(sc->ctx, cudaMalloc(&p, bytes));
-    sc->allocations.push_back(p);
-    sc->bytes += bytes;
-    SPT_CUDA(sc->ctx, cudaMemcpy(p, host.data(), bytes, cudaMemcpyHostToDevice));
-    *dst = static_cast<const T*>(p);
-    return SPT_OK;
-}
+};
+
 
 }  // namespace
 }  // namespace spt
@@ -474,27 +491,28 @@ spt_status spt_scene_create(spt_context* ctx, const spt_scene_desc* d, const spt
         S.has_spheres = any_sphere;
         sc->n_materials = d->n_materials;
         sc->any_emission = any_em;
-        if ((s = upload(sc.get(), tri, &S.tri)) != SPT_OK) return s;
-        if ((s = upload(sc.get(), pair, &S.pair)) != SPT_OK) return s;
-        if ((s = upload(sc.get(), leaf, &S.leaf)) != SPT_OK) return s;
-        if ((s = upload(sc.get(), leaf_box, &S.leaf_box)) != SPT_OK) return s;
-        if ((s = upload(sc.get(), node2, &S.node2)) != SPT_OK) return s;
-        if ((s = upload(sc.get(), face, &S.face_normal)) != SPT_OK) return s;
-        if ((s = upload(sc.get(), smooth, &S.smooth_normal)) != SPT_OK) return s;
-        if ((s = upload(sc.get(), pm, &S.prim_mat)) != SPT_OK) return s;
-        if ((s = upload(sc.get(), pt, &S.prim_type)) != SPT_OK) return s;
-        if ((s = upload(sc.get(), bs, &S.bsdf)) != SPT_OK) return s;
-        if ((s = upload(sc.get(), ms, &S.mat)) != SPT_OK) return s;
-        if ((s = upload(sc.get(), layers, &S.layer_ids)) != SPT_OK) return s;
-        {
-            const uint4* wn = nullptr;
-            std::vector<uint4> raw(wnodes.size() * 5);
-            if (!wnodes.empty()) std::memcpy(raw.data(), wnodes.data(), wnodes.size() * sizeof(WideNode));
-            if ((s = upload(sc.get(), raw, &wn)) != SPT_OK) return s;
-            S.wnode = wn;
-            S.n_wnodes = static_cast<uint32_t>(wnodes.size());
-            if ((s = upload(sc.get(), wtri, &S.wtri)) != SPT_OK) return s;
-        }
+        std::vector<uint4> raw(wnodes.size() * 5);
+        if (!wnodes.empty()) std::memcpy(raw.data(), wnodes.data(), wnodes.size() * sizeof(WideNode));
+        const uint4* wn = nullptr;
+        // every array in one device allocation (one cudaMalloc per scene instead of fourteen)
+        Upload up;
+        up.add(tri, &S.tri);
+        up.add(pair, &S.pair);
+        up.add(leaf, &S.leaf);
+        up.add(leaf_box, &S.leaf_box);
+        up.add(node2, &S.node2);
+        up.add(face, &S.face_normal);
+        up.add(smooth, &S.smooth_normal);
+        up.add(pm, &S.prim_mat);
+        up.add(pt, &S.prim_type);
+        up.add(bs, &S.bsdf);
+        up.add(ms, &S.mat);
+        up.add(layers, &S.layer_ids);
+        up.add(raw, &wn);
+        up.add(wtri, &S.wtri);
+        if ((s = up.commit(sc.get())) != SPT_OK) return s;
+        S.wnode = wn;
+        S.n_wnodes = static_cast<uint32_t>(wnodes.size());
         *out = sc.release();
         return SPT_OK;
     } catch (const std::bad_alloc&) {

@@ -329,21 +329,22 @@ __global__ void k_down_leaves(Nodes N, Tree T, uint32_t n, uint32_t* __restrict_
     }
 }
 
-// Device buffers of one build, freed on every exit path.
-struct Scratch {
-    std::vector<void*> ptrs;
-    ~Scratch() {
-        for (void* p : ptrs) cudaFree(p);
-    }
+// Bump layout of one build's buffers in one region, 256-byte aligned.  A pass with base 0 only sizes
+// the region.
+struct Bump {
+    uintptr_t base;
+    size_t off = 0;
     template <typename T>
-    cudaError_t get(T** p, size_t count) {
-        void* q = nullptr;
-        const cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
-        if (e == cudaSuccess) ptrs.push_back(q);
-        *p = static_cast<T*>(q);
-        return e;
+    void take(T** p, size_t count) {
+        off = (off + 255) & ~static_cast<size_t>(255);
+        *p = reinterpret_cast<T*>(base + off);
+        off += std::max<size_t>(count, 1) * sizeof(T);
     }
 };
+
+// The context's scratch slot that holds a build's buffers; it stays allocated, so later builds of
+// no larger scenes allocate nothing (scenes of a batch are often built back to back).
+constexpr int kBuildSlot = 10;
 
 }  // namespace
 
@@ -356,49 +357,62 @@ spt_status build_ploc_tree(spt_context* ctx, const spt_scene_desc& d, HostBvh& o
     if (n == 0) return SPT_OK;
     if (n > (1u << 30)) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "device BVH build: at most 2^30 primitives");
     cudaStream_t s = ctx->stream;
-    Scratch S;
     float* prim;
     uint8_t* type;
     float4 *bmin, *bmax, *cen;
-    uint32_t *cb, *vals, *vals2, *cur, *cur2, *nn, *next, *keep, *pos, *counters;
+    uint32_t *cb, *vals, *vals2, *cur, *cur2, *nn, *next, *keep, *pos, *counters, *d_refs;
     uint64_t *keys, *keys2;
+    spt_bvh2_node* d_out;
+    char* temp;
     Nodes N;
-    const size_t n_nodes = 2ull * n - 1;
-    SPT_CUDA(ctx, S.get(&prim, 9ull * n));
-    SPT_CUDA(ctx, S.get(&type, n));
-    SPT_CUDA(ctx, S.get(&bmin, n));
-    SPT_CUDA(ctx, S.get(&bmax, n));
-    SPT_CUDA(ctx, S.get(&cen, n));
-    SPT_CUDA(ctx, S.get(&cb, 8));
-    SPT_CUDA(ctx, S.get(&keys, n));
-    SPT_CUDA(ctx, S.get(&keys2, n));
-    SPT_CUDA(ctx, S.get(&vals, n));
-    SPT_CUDA(ctx, S.get(&vals2, n));
-    SPT_CUDA(ctx, S.get(&cur, n));
-    SPT_CUDA(ctx, S.get(&cur2, n));
-    SPT_CUDA(ctx, S.get(&nn, n));
-    SPT_CUDA(ctx, S.get(&next, n));
-    SPT_CUDA(ctx, S.get(&keep, n));
-    SPT_CUDA(ctx, S.get(&pos, n));
-    SPT_CUDA(ctx, S.get(&counters, 2));
-    SPT_CUDA(ctx, S.get(&N.mn, n_nodes));
-    SPT_CUDA(ctx, S.get(&N.mx, n_nodes));
-    SPT_CUDA(ctx, S.get(&N.child, n_nodes));
     Tree T;
-    SPT_CUDA(ctx, S.get(&T.cnt, n_nodes));
-    SPT_CUDA(ctx, S.get(&T.cost, n_nodes));
-    SPT_CUDA(ctx, S.get(&T.col, n_nodes));
-    SPT_CUDA(ctx, S.get(&T.outsize, n_nodes));
-    SPT_CUDA(ctx, S.get(&T.idx, n_nodes));
-    SPT_CUDA(ctx, S.get(&T.rb, n_nodes));
-    SPT_CUDA(ctx, S.get(&T.state, n_nodes));
+    const size_t n_nodes = 2ull * n - 1;
     // sort and scan scratch, sized for the largest call
     size_t sort_bytes = 0, scan_bytes = 0;
-    SPT_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, keys, keys2, vals, vals2,
-                                                  static_cast<int>(n), 0, 63, s));
-    SPT_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, keep, pos, static_cast<int>(n), s));
-    void* temp;
-    SPT_CUDA(ctx, S.get(reinterpret_cast<char**>(&temp), std::max(sort_bytes, scan_bytes)));
+    SPT_CUDA(ctx, cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, static_cast<const uint64_t*>(nullptr),
+                                                  static_cast<uint64_t*>(nullptr), static_cast<const uint32_t*>(nullptr),
+                                                  static_cast<uint32_t*>(nullptr), static_cast<int>(n), 0, 63, s));
+    SPT_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, static_cast<const uint32_t*>(nullptr),
+                                                static_cast<uint32_t*>(nullptr), static_cast<int>(n), s));
+    auto layout = [&](Bump& B) {
+        B.take(&prim, 9ull * n);
+        B.take(&type, n);
+        B.take(&bmin, n);
+        B.take(&bmax, n);
+        B.take(&cen, n);
+        B.take(&cb, 8);
+        B.take(&keys, n);
+        B.take(&keys2, n);
+        B.take(&vals, n);
+        B.take(&vals2, n);
+        B.take(&cur, n);
+        B.take(&cur2, n);
+        B.take(&nn, n);
+        B.take(&next, n);
+        B.take(&keep, n);
+        B.take(&pos, n);
+        B.take(&counters, 2);
+        B.take(&N.mn, n_nodes);
+        B.take(&N.mx, n_nodes);
+        B.take(&N.child, n_nodes);
+        B.take(&T.cnt, n_nodes);
+        B.take(&T.cost, n_nodes);
+        B.take(&T.col, n_nodes);
+        B.take(&T.outsize, n_nodes);
+        B.take(&T.idx, n_nodes);
+        B.take(&T.rb, n_nodes);
+        B.take(&T.state, n_nodes);
+        B.take(&d_out, n_nodes);
+        B.take(&d_refs, n);
+        B.take(&temp, std::max(sort_bytes, scan_bytes));
+    };
+    Bump sizing{0};
+    layout(sizing);
+    void* region;
+    spt_status st = scratch(ctx, kBuildSlot, sizing.off, &region);
+    if (st != SPT_OK) return st;
+    Bump real{reinterpret_cast<uintptr_t>(region)};
+    layout(real);
 
     SPT_CUDA(ctx, cudaMemcpyAsync(prim, d.prim_data, 9ull * n * sizeof(float), cudaMemcpyHostToDevice, s));
     SPT_CUDA(ctx, cudaMemcpyAsync(type, d.prim_type, n, cudaMemcpyHostToDevice, s));
@@ -419,11 +433,7 @@ spt_status build_ploc_tree(spt_context* ctx, const spt_scene_desc& d, HostBvh& o
     uint32_t m = n;
     uint32_t passes = 0;
     uint32_t* h_count;
-    SPT_CUDA(ctx, cudaMallocHost(&h_count, 2 * sizeof(uint32_t)));
-    struct PinnedFree {
-        uint32_t* p;
-        ~PinnedFree() { cudaFreeHost(p); }
-    } pin{h_count};
+    if ((st = pinned(ctx, 2 * sizeof(uint32_t), reinterpret_cast<void**>(&h_count))) != SPT_OK) return st;
     std::vector<uint32_t> bounds{n};   // node ids created by pass p: [bounds[p], bounds[p + 1])
     while (m > 1) {
         if (++passes > n) return fail(ctx, SPT_ERR_INTERNAL, "device BVH build did not converge");
@@ -455,10 +465,6 @@ spt_status build_ploc_tree(spt_context* ctx, const spt_scene_desc& d, HostBvh& o
     SPT_CUDA(ctx, cudaMemcpyAsync(&n_out, T.outsize + root, sizeof(n_out), cudaMemcpyDeviceToHost, s));
     SPT_CUDA(ctx, cudaStreamSynchronize(s));
     if (n_out == 0 || n_out > n_nodes) return fail(ctx, SPT_ERR_INTERNAL, "device BVH build: bad node count");
-    spt_bvh2_node* d_out;
-    uint32_t* d_refs;
-    SPT_CUDA(ctx, S.get(&d_out, n_out));
-    SPT_CUDA(ctx, S.get(&d_refs, n));
     for (size_t p = bounds.size() - 1; p-- > 0;) {
         const uint32_t a = bounds[p], b = bounds[p + 1];
         k_down<<<static_cast<unsigned>(std::min<uint64_t>((b - a + 255) / 256, 8ull * sms)), 256, 0, s>>>(N, T, a, b,

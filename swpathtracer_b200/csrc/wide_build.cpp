@@ -144,8 +144,10 @@ struct Collapser {
     // The wide node idx over `items`: written to out[idx], its leaf triangles appended to rank, its
     // inner children given consecutive slots at the end of out and returned with their items.
     void fill_node(uint32_t idx, const Items& items, Kids& kids) {
-        // expand LEAF items into chunks of up to three triangles
+        // expand LEAF items into chunks of up to three triangles (items is never empty: a binary
+        // node has two children and a leaf at least one reference)
         Items ch;
+        ch.v[0] = items.v[0];
         for (int k = 0; k < items.n; ++k) {
             const Item& it = items.v[k];
             if (it.kind == LEAF)
