@@ -296,7 +296,10 @@ __global__ void __launch_bounds__(256) k_class_scatter(Wave W, const Counters* _
 // SM) runs plain shading 1-3 % faster than the 114 registers it takes unbounded, despite a few
 // spilled bytes, and guided shading as fast as its unbounded 122 (148 with a one-block bound: 7 %
 // slower).
-template <bool GUIDED>
+// RECORDS: the guided render still trains, so paths carry the ids of their open training records and
+// add the emission they find to them.  Once the guide is frozen (the last pass of a guided render,
+// nearly all of its samples) that state is neither read nor written.
+template <bool GUIDED, bool RECORDS>
 __global__ void __launch_bounds__(256, 3) k_shade(Wave W, Counters* __restrict__ ctr, PathBuf cur, PathBuf nxt,
                                                const float4* __restrict__ hits, GuideIO G,
                                                const uint32_t* __restrict__ order) {
@@ -315,7 +318,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(Wave W, Counters* __restrict__
             // evict-first loads leave L2 to the scene
             const float4 o4 = __ldcs(cur.o + i), d4 = __ldcs(cur.d + i), b4 = __ldcs(cur.b + i), l4 = __ldcs(cur.l + i),
                          h4 = __ldcs(hits + i);
-            if (GUIDED) rr = cur.r[i];
+            if (GUIDED && RECORDS) rr = cur.r[i];
             const uint32_t pix = __float_as_uint(o4.w), sg = __float_as_uint(d4.w);
             const uint32_t jd = __float_as_uint(b4.w);
             const int depth = static_cast<int>(jd & 0xFFFFu);
@@ -363,7 +366,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(Wave W, Counters* __restrict__
                 }
                 const V3 no = pos + wwi * 1e-3f;
                 const V3 le = v3(m.er, m.eg, m.eb);
-                if (GUIDED && (le.x != 0.0f || le.y != 0.0f || le.z != 0.0f)) {
+                if (GUIDED && RECORDS && (le.x != 0.0f || le.y != 0.0f || le.z != 0.0f)) {
                     // radiance reaching the path's open training records
                     const V3 add = beta * le;
                     const uint32_t ids[4] = {rr.x, rr.y, rr.z, rr.w};
@@ -389,7 +392,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(Wave W, Counters* __restrict__
                         (!J.rr && depth + 1 >= J.path_length)) {   // the next trace would return 0
                         done = true;
                     } else {
-                        if (GUIDED && gi != kNoRec && c.train_on) {
+                        if (GUIDED && RECORDS && gi != kNoRec && c.train_on) {
                             const uint32_t r = atomicAdd(&ctr->rec_count, 1u);
                             if (r < G.rec_cap) {
                                 G.rec[4ull * r] = make_float4(pos.x, pos.y, pos.z, 0.0f);
@@ -422,7 +425,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(Wave W, Counters* __restrict__
                 nxt.d[slot] = wo_d;
                 nxt.b[slot] = wo_b;
                 nxt.l[slot] = wo_l;
-                if (GUIDED) nxt.r[slot] = rr;
+                if (GUIDED && RECORDS) nxt.r[slot] = rr;
             }
         }
     }
@@ -635,9 +638,10 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
             order = d_order;
         }
         if (guide) {
-            k_shade<true><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
+            if (train_budget > 0) k_shade<true, true><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
+            else k_shade<true, false><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
         } else {
-            k_shade<false><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
+            k_shade<false, false><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
         }
         k_advance<<<1, 1, 0, ctx->stream>>>(W, d_ctr);
     }
