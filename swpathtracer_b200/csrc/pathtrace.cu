@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(128) k_extend_df(Wave W, Counters* __restrict_
     const uint32_t n = c.n_alive + n_new_paths(W, c);
     const uint32_t lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    WideTraversal tr;
+    WideTraversalT<true> tr;
     // the lane's scene, held by value: the fields the traversal reads stay in registers instead of
     // being reloaded from the job table at every node
     DevScene S{};
