@@ -142,10 +142,10 @@ __device__ __forceinline__ Hit1 closest_hit_wide_pass(const DevScene& S, V3 o, V
         }
         if (!g_hits) {
             if (sp == 0) break;
-            --sp;
-            g_base = stack[sp].x;
-            g_hits = stack[sp].y & 0xFFu;
-            g_imask = stack[sp].y >> 8;
+            const uint2 e = stack[--sp];   // one 8-byte load
+            g_base = e.x;
+            g_hits = e.y & 0xFFu;
+            g_imask = e.y >> 8;
         }
         const uint32_t key = __ffs(g_hits) - 1;
         g_hits &= g_hits - 1;
