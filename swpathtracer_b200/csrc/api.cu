@@ -1,6 +1,7 @@
 // api.cu -- context, acceleration structure and scene entry points of the C-ABI (include/spt.h).
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <fstream>
 #include <memory>
 #include <new>
@@ -117,6 +118,25 @@ spt_status make_camera(spt_context* ctx, const spt_camera* c, DevCamera& k) {
 }
 
 namespace {
+
+// f(begin, end) over [0, n) in chunks on the host's threads; for loops whose iterations write
+// disjoint, preallocated outputs (the results do not depend on the split).
+template <typename F>
+void parallel_for(size_t n, F f) {
+    const size_t max_t = std::max(1u, std::thread::hardware_concurrency());
+    const size_t t = std::min(max_t, (n + 65535) / 65536);
+    if (t <= 1) {
+        f(size_t{0}, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const size_t chunk = (n + t - 1) / t;
+    for (size_t k = 0; k < t; ++k) {
+        const size_t a = k * chunk, b = std::min(n, a + chunk);
+        if (a < b) pool.emplace_back(f, a, b);
+    }
+    for (auto& th : pool) th.join();
+}
 
 inline float bits_f(uint32_t u) {
     float f;
@@ -352,20 +372,23 @@ spt_status spt_scene_create(spt_context* ctx, const spt_scene_desc* d, const spt
             any_sphere |= d->prim_type[i] == SPT_PRIM_SPHERE;
         }
         if (any_smooth) smooth.resize(3ull * n);
-        for (uint32_t i = 0; i < n; ++i) {
-            const float* p = d->prim_data + 9ull * i;
-            if (d->prim_type[i] == SPT_PRIM_SPHERE) {
-                face[i] = make_float4(p[0], p[1], p[2], p[3]);
-            } else {
-                V3 v0 = v3(p[0], p[1], p[2]), v1 = v3(p[3], p[4], p[5]), v2 = v3(p[6], p[7], p[8]);
-                V3 nn = normalize(cross(v1 - v0, v2 - v0));  // triangle.cpp:6
-                face[i] = make_float4(nn.x, nn.y, nn.z, 0.0f);
-                if (d->prim_type[i] == SPT_PRIM_SMOOTH_TRIANGLE) {
-                    const float* q = d->prim_normals + 9ull * i;
-                    for (int k = 0; k < 3; ++k) smooth[3ull * i + k] = make_float4(q[3 * k], q[3 * k + 1], q[3 * k + 2], 0.0f);
+        parallel_for(n, [&](size_t a, size_t b) {
+            for (size_t i = a; i < b; ++i) {
+                const float* p = d->prim_data + 9ull * i;
+                if (d->prim_type[i] == SPT_PRIM_SPHERE) {
+                    face[i] = make_float4(p[0], p[1], p[2], p[3]);
+                } else {
+                    V3 v0 = v3(p[0], p[1], p[2]), v1 = v3(p[3], p[4], p[5]), v2 = v3(p[6], p[7], p[8]);
+                    V3 nn = normalize(cross(v1 - v0, v2 - v0));  // triangle.cpp:6
+                    face[i] = make_float4(nn.x, nn.y, nn.z, 0.0f);
+                    if (d->prim_type[i] == SPT_PRIM_SMOOTH_TRIANGLE) {
+                        const float* q = d->prim_normals + 9ull * i;
+                        for (int k = 0; k < 3; ++k)
+                            smooth[3ull * i + k] = make_float4(q[3 * k], q[3 * k + 1], q[3 * k + 2], 0.0f);
+                    }
                 }
             }
-        }
+        });
         // leaf ordinals for the slots (filled below)
         std::vector<uint32_t> slot_leaf(n, 0);
         std::vector<float4> pair;
@@ -381,27 +404,29 @@ spt_status spt_scene_create(spt_context* ctx, const spt_scene_desc* d, const spt
             pair.resize(4ull * n_inner);
             leaf.resize(n_leaf);
             leaf_box.resize(6ull * n_leaf);
-            for (size_t i = 0; i < nn; ++i) {
-                const spt_bvh2_node& nd = nodes[i];
-                if (nd.count) {
-                    int l = ~ord[i];
-                    leaf[l] = make_int2(static_cast<int>(nd.right), static_cast<int>(nd.count));
-                    for (int k = 0; k < 3; ++k) {
-                        leaf_box[6ull * l + k] = nd.min[k];
-                        leaf_box[6ull * l + 3 + k] = nd.max[k];
+            parallel_for(nn, [&](size_t a, size_t b) {   // leaves cover disjoint slot ranges
+                for (size_t i = a; i < b; ++i) {
+                    const spt_bvh2_node& nd = nodes[i];
+                    if (nd.count) {
+                        int l = ~ord[i];
+                        leaf[l] = make_int2(static_cast<int>(nd.right), static_cast<int>(nd.count));
+                        for (int k = 0; k < 3; ++k) {
+                            leaf_box[6ull * l + k] = nd.min[k];
+                            leaf_box[6ull * l + 3 + k] = nd.max[k];
+                        }
+                        for (uint32_t k = 0; k < nd.count; ++k) slot_leaf[nd.right + k] = static_cast<uint32_t>(l);
+                    } else {
+                        const spt_bvh2_node& L = nodes[i + 1];
+                        const spt_bvh2_node& R = nodes[nd.right];
+                        float4* p = &pair[4ull * ord[i]];
+                        p[0] = make_float4(L.min[0], L.min[1], L.min[2], L.max[0]);
+                        p[1] = make_float4(L.max[1], L.max[2], R.min[0], R.min[1]);
+                        p[2] = make_float4(R.min[2], R.max[0], R.max[1], R.max[2]);
+                        int4 refs = make_int4(ord[i + 1], ord[nd.right], 0, 0);
+                        std::memcpy(&p[3], &refs, sizeof(refs));
                     }
-                    for (uint32_t k = 0; k < nd.count; ++k) slot_leaf[nd.right + k] = static_cast<uint32_t>(l);
-                } else {
-                    const spt_bvh2_node& L = nodes[i + 1];
-                    const spt_bvh2_node& R = nodes[nd.right];
-                    float4* p = &pair[4ull * ord[i]];
-                    p[0] = make_float4(L.min[0], L.min[1], L.min[2], L.max[0]);
-                    p[1] = make_float4(L.max[1], L.max[2], R.min[0], R.min[1]);
-                    p[2] = make_float4(R.min[2], R.max[0], R.max[1], R.max[2]);
-                    int4 refs = make_int4(ord[i + 1], ord[nd.right], 0, 0);
-                    std::memcpy(&p[3], &refs, sizeof(refs));
                 }
-            }
+            });
             node2 = nodes;
             S.n_inner = n_inner;
             S.n_leaves = n_leaf;
@@ -418,20 +443,22 @@ spt_status spt_scene_create(spt_context* ctx, const spt_scene_desc* d, const spt
             leaf_box.assign(6, 0.0f);
             S.n_leaves = 1;
         }
-        for (uint32_t s2 = 0; s2 < n; ++s2) {
-            const uint32_t i = slot_prim[s2];
-            const float* p = d->prim_data + 9ull * i;
-            float4* r = &tri[3ull * s2];
-            if (d->prim_type[i] == SPT_PRIM_SPHERE) {
-                r[0] = make_float4(p[0], p[1], p[2], bits_f(i));
-                r[1] = make_float4(p[3], 0.0f, 0.0f, bits_f(slot_leaf[s2]));
-                r[2] = make_float4(0.0f, 0.0f, 0.0f, bits_f(SPT_PRIM_SPHERE));
-            } else {
-                r[0] = make_float4(p[0], p[1], p[2], bits_f(i));
-                r[1] = make_float4(p[3] - p[0], p[4] - p[1], p[5] - p[2], bits_f(slot_leaf[s2]));
-                r[2] = make_float4(p[6] - p[0], p[7] - p[1], p[8] - p[2], bits_f(d->prim_type[i]));
+        parallel_for(n, [&](size_t a, size_t b) {
+            for (size_t s2 = a; s2 < b; ++s2) {
+                const uint32_t i = slot_prim[s2];
+                const float* p = d->prim_data + 9ull * i;
+                float4* r = &tri[3ull * s2];
+                if (d->prim_type[i] == SPT_PRIM_SPHERE) {
+                    r[0] = make_float4(p[0], p[1], p[2], bits_f(i));
+                    r[1] = make_float4(p[3], 0.0f, 0.0f, bits_f(slot_leaf[s2]));
+                    r[2] = make_float4(0.0f, 0.0f, 0.0f, bits_f(SPT_PRIM_SPHERE));
+                } else {
+                    r[0] = make_float4(p[0], p[1], p[2], bits_f(i));
+                    r[1] = make_float4(p[3] - p[0], p[4] - p[1], p[5] - p[2], bits_f(slot_leaf[s2]));
+                    r[2] = make_float4(p[6] - p[0], p[7] - p[1], p[8] - p[2], bits_f(d->prim_type[i]));
+                }
             }
-        }
+        });
         // 8-wide quantized tree over the same leaves (traverse_wide.cuh)
         std::vector<WideNode> wnodes;
         std::vector<float4> wtri;
@@ -440,20 +467,22 @@ spt_status spt_scene_create(spt_context* ctx, const spt_scene_desc* d, const spt
             build_wide(tree->nodes, wb);
             wnodes.swap(wb.nodes);
             wtri.resize(3ull * wb.tri_rank.size());
-            for (size_t k = 0; k < wb.tri_rank.size(); ++k) {
-                const uint32_t rk = wb.tri_rank[k];
-                const float4* r = &tri[3ull * rk];
-                const uint32_t type = d->prim_type[slot_prim[rk]];
-                if (type == SPT_PRIM_SPHERE) {
-                    wtri[3 * k] = make_float4(r[0].x, r[0].y, r[0].z, bits_f(rk));
-                    wtri[3 * k + 1] = make_float4(0.0f, 0.0f, 0.0f, bits_f(type));
-                    wtri[3 * k + 2] = make_float4(r[1].x, 0.0f, 0.0f, r[1].w);
-                } else {
-                    wtri[3 * k] = make_float4(r[0].x, r[0].y, r[0].z, bits_f(rk));
-                    wtri[3 * k + 1] = make_float4(r[1].x, r[1].y, r[1].z, bits_f(type));
-                    wtri[3 * k + 2] = make_float4(r[2].x, r[2].y, r[2].z, r[1].w);  // leaf id
+            parallel_for(wb.tri_rank.size(), [&](size_t a, size_t b) {
+                for (size_t k = a; k < b; ++k) {
+                    const uint32_t rk = wb.tri_rank[k];
+                    const float4* r = &tri[3ull * rk];
+                    const uint32_t type = d->prim_type[slot_prim[rk]];
+                    if (type == SPT_PRIM_SPHERE) {
+                        wtri[3 * k] = make_float4(r[0].x, r[0].y, r[0].z, bits_f(rk));
+                        wtri[3 * k + 1] = make_float4(0.0f, 0.0f, 0.0f, bits_f(type));
+                        wtri[3 * k + 2] = make_float4(r[1].x, 0.0f, 0.0f, r[1].w);
+                    } else {
+                        wtri[3 * k] = make_float4(r[0].x, r[0].y, r[0].z, bits_f(rk));
+                        wtri[3 * k + 1] = make_float4(r[1].x, r[1].y, r[1].z, bits_f(type));
+                        wtri[3 * k + 2] = make_float4(r[2].x, r[2].y, r[2].z, r[1].w);  // leaf id
+                    }
                 }
-            }
+            });
             const char* env = std::getenv("SPT_TRAVERSAL");
             S.traversal = 2;  // wide nodes, persistent dynamic fetch where a kernel supports it
             if (env && std::string(env) == "binary") S.traversal = 0;

@@ -42,15 +42,21 @@ def test_guided_render_is_unbiased_and_less_noisy(device, small_light):
     gs, cam, ref = small_light
     p = scenes.pt_params(spp=1024, path_length=5, seed=7)
     plain, _ = _render(gs, cam, p)
-    g = spt.Guide(device, spt.guide_config(batch=1 << 16, max_steps=64, mix=0.5, seed=1))
-    guided, st = _render(gs, cam, p, g)
-    assert g.steps > 0
-    assert np.isfinite(guided).all()
-    assert st.paths == 64 * 64 * 1024
-    # the image mean's relative standard error is about 0.7 % at 1024 spp here
-    assert abs(float(guided.mean()) - float(ref.mean())) <= 0.03 * float(ref.mean())
-    e_plain, e_guided = relmse(plain, ref), relmse(guided, ref)
-    assert e_guided < 1.3 * e_plain, (e_guided, e_plain)
+    e_plain = relmse(plain, ref)
+    # Training sums gradients with float atomics, so a guide's quality varies from run to run: one
+    # guide's relMSE ranged over 0.82-1.33x the plain render's on this scene; two guides are averaged.
+    e_guided = []
+    for seed in (1, 2):
+        g = spt.Guide(device, spt.guide_config(batch=1 << 16, max_steps=64, mix=0.5, seed=seed))
+        guided, st = _render(gs, cam, p, g)
+        assert g.steps > 0
+        assert np.isfinite(guided).all()
+        assert st.paths == 64 * 64 * 1024
+        # the image mean's relative standard error is about 0.7 % at 1024 spp here
+        assert abs(float(guided.mean()) - float(ref.mean())) <= 0.03 * float(ref.mean())
+        e_guided.append(relmse(guided, ref))
+        g.close()
+    assert np.mean(e_guided) < 1.3 * e_plain, (e_guided, e_plain)
 
 
 @pytest.mark.parametrize("mix", [0.5, 0.9])
