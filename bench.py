@@ -392,7 +392,9 @@ def main():
            "bvh_build_ms": round(build_ms, 1),
            "clocks": clk}
 
-    if rank == 0 and not a.no_extras:
+    # the submetrics are single-GPU measurements: under torchrun (N > 1) they would hold every rank's
+    # GPU for minutes while only rank 0 works, so they run at N = 1 only
+    if rank == 0 and world == 1 and not a.no_extras:
         extras = {}
         for name, mode in (("normal", abi.RAYCAST_NORMAL), ("depth", abi.RAYCAST_DEPTH), ("count", abi.RAYCAST_COUNT)):
             cam = scenes.displaced_mesh_camera(1920, 1080)
