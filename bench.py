@@ -477,7 +477,7 @@ def main():
         # guided rendering: a room lit through a 0.1 x 0.1 window (directional transport), and the
         # small-light box (light found mostly via a two-sided emitter's halo; guiding loses there)
         extras.update(guided_vs_plain(spt, scenes, dev, torch, "guided_window_room_128x128",
-                                      scenes.window_room_scene(0.1), 16384, 262144, 32))
+                                      scenes.window_room_scene(0.1), 16384, 262144, 32, seeds=tuple(range(7, 15))))
         extras.update(guided_vs_plain(spt, scenes, dev, torch, "guided_small_light_128x128",
                                       scenes.small_light_box_scene(), 4096, 16384, 32, seeds=(7,)))
         # guided rendering on a sample of the batch set (box with a 0.25 x 0.25 ceiling light)
