@@ -142,7 +142,9 @@ class GpuScene:
 
     # ---- ray queries -------------------------------------------------------------------------
     def intersect(self, rays, counts=False, out=None, out_counts=None):
-        """Closest hit per ray (rays: float32 [n, 8]); counts adds the reference's per-ray test counts.
+        """Closest hit per ray (rays: float32 [n, 8] = origin, 0, direction, 0; or [n, 6] = the reference's
+        Ray layout, origin then direction, through spt_intersect_packed); counts adds the reference's
+        per-ray test counts.
         out: optional preallocated (e.g. pinned) array of abi.HIT_DTYPE for the hits; out_counts:
         optional (tests, nhits) uint32 arrays for the counts.  With every buffer page-locked, large
         batches run as a pipeline of chunks whose copies overlap the queries."""
@@ -156,9 +158,11 @@ class GpuScene:
         else:
             tests = np.zeros(n, np.uint32) if counts else None
             nh = np.zeros(n, np.uint32) if counts else None
-        self.dev.check(self.lib.spt_intersect(self.dev.h, self.h, rays.ctypes.data, n, hits.ctypes.data,
-                                              None if tests is None else tests.ctypes.data,
-                                              None if nh is None else nh.ctypes.data), "spt_intersect")
+        assert rays.ndim == 2 and rays.shape[1] in (6, 8)
+        fn = self.lib.spt_intersect_packed if rays.shape[1] == 6 else self.lib.spt_intersect
+        self.dev.check(fn(self.dev.h, self.h, rays.ctypes.data, n, hits.ctypes.data,
+                          None if tests is None else tests.ctypes.data, None if nh is None else nh.ctypes.data),
+                       "spt_intersect")
         return dict(hits=hits, tests=tests, nhits=nh)
 
     def intersect_noalloc(self, rays, counts=False):

@@ -16,33 +16,49 @@ namespace {
 
 constexpr int kBlock = 128;
 
+// Ray i of a batch in either host layout: STRIDE 8 = {origin, pad, direction, pad} as two float4;
+// STRIDE 6 = the reference's Ray (core/ray.h: two glm::vec3, 24 bytes) as three float2.  STREAM
+// reads with the evict-first hint (rays are read once).
+template <int STRIDE, bool STREAM>
+__device__ __forceinline__ void load_ray(const float* __restrict__ rays, uint64_t i, V3& o, V3& d) {
+    if (STRIDE == 8) {
+        const float4* r = reinterpret_cast<const float4*>(rays) + 2 * i;
+        const float4 a = STREAM ? __ldcs(r) : __ldg(r), b = STREAM ? __ldcs(r + 1) : __ldg(r + 1);
+        o = f3v(a);
+        d = f3v(b);
+    } else {
+        const float2* r = reinterpret_cast<const float2*>(rays) + 3 * i;
+        const float2 a = STREAM ? __ldcs(r) : __ldg(r), b = STREAM ? __ldcs(r + 1) : __ldg(r + 1),
+                     c = STREAM ? __ldcs(r + 2) : __ldg(r + 2);
+        o = v3(a.x, a.y, b.x);
+        d = v3(b.y, c.x, c.y);
+    }
+}
+
 // Persistent variant: wide traversal, lanes refilled from a global ray counter (traverse_wide.cuh).
 // 10 blocks of 128 per SM (at most 48 registers): 40 resident warps to hide the node-fetch latency.
 // Rays are read and hits written once, with the evict-first (streaming) cache hint, so the ray and
 // hit streams (48 B per ray, 768 MB per 2^24 rays) push less of the scene out of L2: +1 %.
-__global__ void __launch_bounds__(kBlock, 10) k_intersect_df(DevScene S, const float4* __restrict__ rays, uint64_t n,
+template <int STRIDE>
+__global__ void __launch_bounds__(kBlock, 10) k_intersect_df(DevScene S, const float* __restrict__ rays, uint64_t n,
                                                          spt_hit* __restrict__ hits, uint32_t* status,
                                                          unsigned long long* next) {
     persistent_trace(
-        S, n, next, status,
-        [&](uint64_t i, V3& o, V3& d) {
-            const float4 a = __ldcs(rays + 2 * i), b = __ldcs(rays + 2 * i + 1);
-            o = f3v(a);
-            d = f3v(b);
-        },
+        S, n, next, status, [&](uint64_t i, V3& o, V3& d) { load_ray<STRIDE, true>(rays, i, o, d); },
         [&](uint64_t i, const Hit1& h) {
             __stcs(reinterpret_cast<float4*>(hits + i),
                    make_float4(h.t, __uint_as_float(h.found ? slot_prim(S, h.slot) : SPT_MISS), h.u, h.v));
         });
 }
 
-template <int TRAV>
-__global__ void __launch_bounds__(kBlock) k_intersect(DevScene S, const float4* __restrict__ rays, uint64_t n,
+template <int TRAV, int STRIDE>
+__global__ void __launch_bounds__(kBlock) k_intersect(DevScene S, const float* __restrict__ rays, uint64_t n,
                                                       spt_hit* __restrict__ hits, uint32_t* status) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
-    Hit1 h = trace_closest<TRAV>(S, f3v(a), f3v(b), status);
+    V3 ro, rd;
+    load_ray<STRIDE, false>(rays, i, ro, rd);
+    Hit1 h = trace_closest<TRAV>(S, ro, rd, status);
     spt_hit o;
     o.t = h.t;
     o.prim_id = h.found ? slot_prim(S, h.slot) : SPT_MISS;
@@ -51,15 +67,17 @@ __global__ void __launch_bounds__(kBlock) k_intersect(DevScene S, const float4* 
     hits[i] = o;
 }
 
-__global__ void __launch_bounds__(kBlock) k_count(DevScene S, const float4* __restrict__ rays, uint64_t n,
+template <int STRIDE>
+__global__ void __launch_bounds__(kBlock) k_count(DevScene S, const float* __restrict__ rays, uint64_t n,
                                                   spt_hit* __restrict__ ref_hits, uint32_t* __restrict__ tests,
                                                   uint32_t* __restrict__ nhits, uint32_t* __restrict__ prim_tests,
                                                   uint32_t* status) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float4 a = __ldg(rays + 2 * i), b = __ldg(rays + 2 * i + 1);
+    V3 ro, rd;
+    load_ray<STRIDE, false>(rays, i, ro, rd);
     CountOut c;
-    Hit1 h = count_traverse<kStack>(S, f3v(a), f3v(b), c, status);
+    Hit1 h = count_traverse<kStack>(S, ro, rd, c, status);
     if (ref_hits) {
         spt_hit o;
         o.t = h.t;
@@ -159,26 +177,41 @@ inline unsigned blocks_for(uint64_t n, int block) { return static_cast<unsigned>
 
 }  // namespace
 
-spt_status launch_intersect(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
-                            cudaStream_t s) {
-    if (n == 0) return SPT_OK;
-    if (n > (1ull << 36)) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "too many rays in one call");
+namespace {
+
+// the persistent kernel's grid (one computation per ray layout)
+template <int STRIDE>
+int df_grid(spt_context* ctx) {
+    static int grid = 0;
+    if (!grid) grid = persistent_grid(ctx, reinterpret_cast<const void*>(k_intersect_df<STRIDE>), kBlock);
+    return grid;
+}
+
+template <int STRIDE>
+spt_status launch_intersect_t(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
+                              cudaStream_t s) {
     if (sc->dev.traversal == 2) {
         unsigned long long* next = nullptr;
         spt_status st = fetch_counter(ctx, s, &next);
         if (st != SPT_OK) return st;
-        static int grid = 0;
-        if (!grid) grid = persistent_grid(ctx, reinterpret_cast<const void*>(k_intersect_df), kBlock);
-        k_intersect_df<<<grid, kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n, d_hits,
-                                              ctx->d_status, next);
-    } else if (sc->dev.traversal == 1)
-        k_intersect<1><<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n,
-                                                                d_hits, ctx->d_status);
-    else
-        k_intersect<0><<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n,
-                                                                d_hits, ctx->d_status);
+        k_intersect_df<STRIDE><<<df_grid<STRIDE>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status, next);
+    } else if (sc->dev.traversal == 1) {
+        k_intersect<1, STRIDE><<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status);
+    } else {
+        k_intersect<0, STRIDE><<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status);
+    }
     SPT_CUDA(ctx, cudaGetLastError());
     return SPT_OK;
+}
+
+}  // namespace
+
+spt_status launch_intersect(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
+                            cudaStream_t s, int stride) {
+    if (n == 0) return SPT_OK;
+    if (n > (1ull << 36)) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "too many rays in one call");
+    if (stride == 6) return launch_intersect_t<6>(ctx, sc, d_rays, n, d_hits, s);
+    return launch_intersect_t<8>(ctx, sc, d_rays, n, d_hits, s);
 }
 
 // launch_intersect with the persistent kernel's ray counter supplied by the caller (zeroed on stream s
@@ -187,20 +220,21 @@ spt_status launch_intersect_fixed(spt_context* ctx, const spt_scene* sc, const f
                                   spt_hit* d_hits, unsigned long long* next, cudaStream_t s) {
     if (n == 0) return SPT_OK;
     if (sc->dev.traversal != 2) return launch_intersect(ctx, sc, d_rays, n, d_hits, s);  // no counter needed
-    static int grid = 0;
-    if (!grid) grid = persistent_grid(ctx, reinterpret_cast<const void*>(k_intersect_df), kBlock);
-    k_intersect_df<<<grid, kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n, d_hits, ctx->d_status,
-                                          next);
+    k_intersect_df<8><<<df_grid<8>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status, next);
     SPT_CUDA(ctx, cudaGetLastError());
     return SPT_OK;
 }
 
 spt_status launch_count(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_ref_hits,
-                        uint32_t* d_tests, uint32_t* d_hits, uint32_t* d_prim_tests, cudaStream_t s) {
+                        uint32_t* d_tests, uint32_t* d_hits, uint32_t* d_prim_tests, cudaStream_t s, int stride) {
     if (n == 0) return SPT_OK;
     if (n > (1ull << 36)) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "too many rays in one call");
-    k_count<<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, reinterpret_cast<const float4*>(d_rays), n, d_ref_hits,
-                                                     d_tests, d_hits, d_prim_tests, ctx->d_status);
+    if (stride == 6)
+        k_count<6><<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, d_rays, n, d_ref_hits, d_tests, d_hits,
+                                                            d_prim_tests, ctx->d_status);
+    else
+        k_count<8><<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, d_rays, n, d_ref_hits, d_tests, d_hits,
+                                                            d_prim_tests, ctx->d_status);
     SPT_CUDA(ctx, cudaGetLastError());
     return SPT_OK;
 }
@@ -244,9 +278,10 @@ bool is_pinned(const void* p) {
 // device buffers; its chunks are in stream order, so a set is reused only after its last chunk's
 // copy out.
 spt_status intersect_pipelined(spt_context* ctx, const spt_scene* sc, const float* rays, uint64_t n, spt_hit* hits,
-                               uint32_t* tests, uint32_t* nhits) {
+                               uint32_t* tests, uint32_t* nhits, int stride) {
     const int P = spt_context::kPipe;
-    const size_t set_bytes = kPipeChunk * (32 + sizeof(spt_hit) + 4 + 4);
+    const uint64_t ray_bytes = 4ull * stride;
+    const size_t set_bytes = kPipeChunk * (ray_bytes + sizeof(spt_hit) + 4 + 4);
     void* mem;
     spt_status st = scratch(ctx, 9, set_bytes * P, &mem);
     if (st != SPT_OK) return st;
@@ -259,15 +294,16 @@ spt_status intersect_pipelined(spt_context* ctx, const spt_scene* sc, const floa
         cudaStream_t s = ctx->pipe[i];
         char* base = static_cast<char*>(mem) + set_bytes * i;
         float* d_rays = reinterpret_cast<float*>(base);
-        spt_hit* d_hits = reinterpret_cast<spt_hit*>(base + kPipeChunk * 32);
-        uint32_t* d_tests = reinterpret_cast<uint32_t*>(base + kPipeChunk * (32 + sizeof(spt_hit)));
+        spt_hit* d_hits = reinterpret_cast<spt_hit*>(base + kPipeChunk * ray_bytes);
+        uint32_t* d_tests = reinterpret_cast<uint32_t*>(base + kPipeChunk * (ray_bytes + sizeof(spt_hit)));
         uint32_t* d_nh = d_tests + kPipeChunk;
         const uint64_t first = c * kPipeChunk, m = std::min(kPipeChunk, n - first);
-        SPT_CUDA(ctx, cudaMemcpyAsync(d_rays, rays + 8 * first, m * 32, cudaMemcpyHostToDevice, s));
-        if ((st = launch_intersect(ctx, sc, d_rays, m, d_hits, s)) != SPT_OK) return st;
+        SPT_CUDA(ctx, cudaMemcpyAsync(d_rays, rays + static_cast<uint64_t>(stride) * first, m * ray_bytes,
+                                      cudaMemcpyHostToDevice, s));
+        if ((st = launch_intersect(ctx, sc, d_rays, m, d_hits, s, stride)) != SPT_OK) return st;
         if (tests || nhits)
             if ((st = launch_count(ctx, sc, d_rays, m, nullptr, tests ? d_tests : nullptr, nhits ? d_nh : nullptr,
-                                   nullptr, s)) != SPT_OK)
+                                   nullptr, s, stride)) != SPT_OK)
                 return st;
         SPT_CUDA(ctx, cudaMemcpyAsync(hits + first, d_hits, m * sizeof(spt_hit), cudaMemcpyDeviceToHost, s));
         if (tests) SPT_CUDA(ctx, cudaMemcpyAsync(tests + first, d_tests, m * 4, cudaMemcpyDeviceToHost, s));
@@ -281,6 +317,36 @@ spt_status intersect_pipelined(spt_context* ctx, const spt_scene* sc, const floa
     return check_status(ctx);
 }
 
+// spt_intersect / spt_intersect_packed: stride floats per host ray.
+spt_status intersect_host(spt_context* ctx, const spt_scene* sc, const float* rays, uint64_t n, spt_hit* hits,
+                          uint32_t* tests, uint32_t* nhits, int stride) {
+    if (!ctx || !sc || (n && (!rays || !hits))) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0) return SPT_OK;
+    SPT_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (n > kPipeChunk && is_pinned(rays) && is_pinned(hits) && (!tests || is_pinned(tests)) &&
+        (!nhits || is_pinned(nhits)))
+        return intersect_pipelined(ctx, sc, rays, n, hits, tests, nhits, stride);
+    spt_status st;
+    void *d_rays, *d_hits, *d_tests = nullptr, *d_nh = nullptr;
+    const uint64_t ray_bytes = 4ull * stride;
+    if ((st = scratch(ctx, 0, n * ray_bytes, &d_rays)) != SPT_OK) return st;
+    if ((st = scratch(ctx, 1, n * sizeof(spt_hit), &d_hits)) != SPT_OK) return st;
+    if (tests && (st = scratch(ctx, 2, n * 4, &d_tests)) != SPT_OK) return st;
+    if (nhits && (st = scratch(ctx, 3, n * 4, &d_nh)) != SPT_OK) return st;
+    SPT_CUDA(ctx, cudaMemcpyAsync(d_rays, rays, n * ray_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    if ((st = launch_intersect(ctx, sc, static_cast<float*>(d_rays), n, static_cast<spt_hit*>(d_hits), ctx->stream,
+                               stride)) != SPT_OK)
+        return st;
+    if (tests || nhits)
+        if ((st = launch_count(ctx, sc, static_cast<float*>(d_rays), n, nullptr, static_cast<uint32_t*>(d_tests),
+                               static_cast<uint32_t*>(d_nh), nullptr, ctx->stream, stride)) != SPT_OK)
+            return st;
+    SPT_CUDA(ctx, cudaMemcpyAsync(hits, d_hits, n * sizeof(spt_hit), cudaMemcpyDeviceToHost, ctx->stream));
+    if (tests) SPT_CUDA(ctx, cudaMemcpyAsync(tests, d_tests, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    if (nhits) SPT_CUDA(ctx, cudaMemcpyAsync(nhits, d_nh, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    return check_status(ctx);
+}
+
 }  // namespace
 }  // namespace spt
 
@@ -290,29 +356,12 @@ extern "C" {
 
 spt_status spt_intersect(spt_context* ctx, const spt_scene* sc, const float* rays, uint64_t n, spt_hit* hits,
                          uint32_t* tests, uint32_t* nhits) {
-    if (!ctx || !sc || (n && (!rays || !hits))) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
-    if (n == 0) return SPT_OK;
-    SPT_CUDA(ctx, cudaSetDevice(ctx->device));
-    if (n > kPipeChunk && is_pinned(rays) && is_pinned(hits) && (!tests || is_pinned(tests)) &&
-        (!nhits || is_pinned(nhits)))
-        return intersect_pipelined(ctx, sc, rays, n, hits, tests, nhits);
-    spt_status st;
-    void *d_rays, *d_hits, *d_tests = nullptr, *d_nh = nullptr;
-    if ((st = scratch(ctx, 0, n * 32, &d_rays)) != SPT_OK) return st;
-    if ((st = scratch(ctx, 1, n * sizeof(spt_hit), &d_hits)) != SPT_OK) return st;
-    if (tests && (st = scratch(ctx, 2, n * 4, &d_tests)) != SPT_OK) return st;
-    if (nhits && (st = scratch(ctx, 3, n * 4, &d_nh)) != SPT_OK) return st;
-    SPT_CUDA(ctx, cudaMemcpyAsync(d_rays, rays, n * 32, cudaMemcpyHostToDevice, ctx->stream));
-    if ((st = launch_intersect(ctx, sc, static_cast<float*>(d_rays), n, static_cast<spt_hit*>(d_hits), ctx->stream)) != SPT_OK)
-        return st;
-    if (tests || nhits)
-        if ((st = launch_count(ctx, sc, static_cast<float*>(d_rays), n, nullptr, static_cast<uint32_t*>(d_tests),
-                               static_cast<uint32_t*>(d_nh), nullptr, ctx->stream)) != SPT_OK)
-            return st;
-    SPT_CUDA(ctx, cudaMemcpyAsync(hits, d_hits, n * sizeof(spt_hit), cudaMemcpyDeviceToHost, ctx->stream));
-    if (tests) SPT_CUDA(ctx, cudaMemcpyAsync(tests, d_tests, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    if (nhits) SPT_CUDA(ctx, cudaMemcpyAsync(nhits, d_nh, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-    return check_status(ctx);
+    return intersect_host(ctx, sc, rays, n, hits, tests, nhits, 8);
+}
+
+spt_status spt_intersect_packed(spt_context* ctx, const spt_scene* sc, const float* rays, uint64_t n, spt_hit* hits,
+                                uint32_t* tests, uint32_t* nhits) {
+    return intersect_host(ctx, sc, rays, n, hits, tests, nhits, 6);
 }
 
 spt_status spt_intersect_device(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n,

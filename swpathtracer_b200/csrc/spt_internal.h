@@ -73,10 +73,11 @@ spt_status check_status(spt_context* ctx);
 spt_status make_camera(spt_context* ctx, const spt_camera* cam, DevCamera& out);
 
 // Kernel launchers (raycast.cu)
+// stride: floats per ray, 8 ({origin, pad, direction, pad}) or 6 (the reference's Ray, core/ray.h)
 spt_status launch_intersect(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
-                            cudaStream_t s);
+                            cudaStream_t s, int stride = 8);
 spt_status launch_count(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_ref_hits,
-                        uint32_t* d_tests, uint32_t* d_hits, uint32_t* d_prim_tests, cudaStream_t s);
+                        uint32_t* d_tests, uint32_t* d_hits, uint32_t* d_prim_tests, cudaStream_t s, int stride = 8);
 
 constexpr int kStack = 64;
 constexpr uint32_t kFetchRing = 1024;

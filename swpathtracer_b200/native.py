@@ -27,6 +27,7 @@ PROTOTYPES = {
     "spt_scene_destroy": (i32, [vp]),
     "spt_scene_device_bytes": (u64, [vp]),
     "spt_intersect": (i32, [vp, vp, vp, u64, vp, vp, vp]),
+    "spt_intersect_packed": (i32, [vp, vp, vp, u64, vp, vp, vp]),
     "spt_intersect_device": (i32, [vp, vp, vp, u64, vp, vp]),
     "spt_count_device": (i32, [vp, vp, vp, u64, vp, vp, vp, vp, vp]),
     "spt_intersect_noalloc": (i32, [vp, vp, vp, u64, vp, vp, vp]),

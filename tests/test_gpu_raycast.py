@@ -142,3 +142,26 @@ def test_pipelined_host_queries_match_device_queries(device):
     assert a["hits"].tobytes() == b["hits"].tobytes()
     np.testing.assert_array_equal(a["tests"], b["tests"])
     np.testing.assert_array_equal(a["nhits"], b["nhits"])
+
+
+def test_reference_ray_layout_matches_padded_layout(device):
+    """spt_intersect_packed takes rays as the reference's Ray lies in memory (origin then direction,
+    24 bytes): the same hits and counts as the padded layout, on the pageable path, the pipelined
+    page-locked path (chunks of 2^20 rays, the last partial) and an empty batch."""
+    import torch
+    packed = scenes.displaced_mesh_scene(6).build()
+    gs = spt.GpuScene(device, packed)
+    n = (1 << 21) + 4321
+    rays8 = scenes.incoherent_rays(n, seed=78, half_extent=1.5)
+    rays6 = np.ascontiguousarray(np.concatenate([rays8[:, 0:3], rays8[:, 4:7]], axis=1))
+    small8, small6 = rays8[:50000], np.ascontiguousarray(rays6[:50000])
+    a = gs.intersect(small8, counts=True)
+    b = gs.intersect(small6, counts=True)
+    assert a["hits"].tobytes() == b["hits"].tobytes()
+    np.testing.assert_array_equal(a["tests"], b["tests"])
+    np.testing.assert_array_equal(a["nhits"], b["nhits"])
+    h6 = torch.from_numpy(rays6).pin_memory().numpy()
+    h_hits = torch.empty((n, 4), dtype=torch.int32).pin_memory().numpy().view(abi.HIT_DTYPE).reshape(n)
+    got = gs.intersect(h6, out=h_hits)
+    assert got["hits"].tobytes() == gs.intersect(rays8)["hits"].tobytes()
+    assert gs.intersect(rays6[:0])["hits"].shape == (0,)
