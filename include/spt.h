@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define SPT_ABI_VERSION 1u
+#define SPT_ABI_VERSION 2u
 #define SPT_MISS 0xFFFFFFFFu
 
 typedef enum spt_status {
@@ -231,6 +231,14 @@ spt_status spt_count_device(spt_context* ctx, const spt_scene* scene, const floa
                             uint64_t n, spt_hit* d_ref_hits, uint32_t* d_tests, uint32_t* d_hits,
                             uint32_t* d_prim_tests, void* stream);
 
+/* The work of the closest-hit kernel itself (no reference counterpart; the reference's own work per
+ * ray is what spt_count_device counts): spt_intersect_device's persistent kernel on n device rays
+ * (8 floats each), with work[0] = 8-wide node visits (each tests up to eight child boxes) and
+ * work[1] = primitive tests, summed over the rays.  The hits are the same as spt_intersect_device's.
+ * Returns after the counts are in host memory. */
+spt_status spt_traversal_work_device(spt_context* ctx, const spt_scene* scene, const float* d_rays, uint64_t n,
+                                     spt_hit* d_hits, uint64_t* work);
+
 /* ---- integrators (reference integrators/integrator.h:8-55) ----------------------------- */
 /* Ray casters, one ray per pixel centre (integrators/raycaster.h:62-99).  out_host layout:
  * NORMAL float[h][w][3] (0 on a miss), DEPTH float[h][w] (-1 on a miss), COUNT int64[h][w]. */
@@ -255,10 +263,18 @@ typedef struct spt_tune {
     uint32_t extend_block;  /* threads per block of the non-persistent extend kernel */
     uint32_t shade_block;   /* threads per block of the shade kernel */
     int32_t traversal;      /* -1 scene default, 0 binary pair nodes, 1 8-wide, 2 8-wide + dynamic fetch */
-    uint32_t check_every;   /* wavefront iterations between host checks for completion */
+    uint32_t check_every;   /* guided renders that train: wavefront iterations between the host's looks
+                               at the training records.  Every other render runs its whole loop on the
+                               device (a conditional WHILE node of one CUDA graph) */
     uint32_t sort_shading;  /* shade the paths grouped by material class: 0 when a scene has layered
                                materials (their walks diverge most), 1 always, 2 never */
-    uint32_t reserved[2];
+    uint32_t stack;         /* traversal stack depth per lane of the persistent extend kernel: 16, 24 or
+                               32 entries; 0 = the smallest that holds every scene's 8-wide tree */
+    uint32_t stack_limit;   /* stack entries a lane may use (0 = all of `stack`); a traversal that needs
+                               more ends the render with SPT_ERR_OVERFLOW */
+    uint32_t max_iterations;/* wavefront iterations before the render gives up with SPT_ERR_TIMEOUT;
+                               0 = a bound from the path count and the 1000-bounce roulette cap */
+    uint32_t reserved;      /* must be 0 */
 } spt_tune;
 
 typedef struct spt_batch_job {
@@ -284,6 +300,8 @@ spt_status spt_autotune(spt_context* ctx, const spt_batch_job* jobs, uint32_t n_
  * a 4-hidden-layer ReLU MLP of width 64 (bf16 tensor-core GEMMs, fp32 accumulation) maps it with the
  * normal and outgoing direction to 8 von Mises-Fisher lobes.  Trained online by Adam on the
  * radiance the path tracer itself collects. */
+enum { SPT_GUIDE_TRAIN_TCGEN05 = 0, SPT_GUIDE_TRAIN_MMA_SYNC = 1 };
+
 typedef struct spt_guide_config {
     float box_min[3], box_max[3];  /* positions are normalised by this box (e.g. the scene bounds) */
     float lr;                      /* Adam learning rate */
@@ -292,7 +310,10 @@ typedef struct spt_guide_config {
     float mix;                     /* probability of sampling the guiding distribution */
     uint64_t seed;                 /* parameter initialisation */
     uint32_t cache_res;            /* cells per axis of the lobe cache guided renders sample: 4..64, 0 = 32 */
-    uint32_t reserved;             /* must be 0 */
+    uint32_t train_path;           /* SPT_GUIDE_TRAIN_TCGEN05 (0): the MLP's training GEMMs on the 5th-gen
+                                      tensor cores, tiles of 128 records with fp32 accumulators in tensor
+                                      memory; SPT_GUIDE_TRAIN_MMA_SYNC (1): warp-level mma.sync tiles of
+                                      32 records */
 } spt_guide_config;
 
 /* One training record: a scattering event and the radiance it led to. */

@@ -13,8 +13,9 @@
  *   - the static buffer is shared by every context of the process on that device: calls that overlap
  *     in time on one device (from two threads, or on two contexts' streams) race on it, so the caller
  *     serialises them;
- *   - the first call on a device looks the buffer up (cudaGetSymbolAddress, which may load the
- *     library's module): make it before any stream capture starts on that device.
+ *   - the first call with a context looks the buffer up (cudaGetSymbolAddress, which may load the
+ *     library's module) and keeps its address in the context: make that call before any stream
+ *     capture starts on the device.
  */
 #ifndef SPT_NOALLOC_H
 #define SPT_NOALLOC_H

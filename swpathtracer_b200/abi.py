@@ -5,7 +5,8 @@ reference interface each one replaces.
 """
 import ctypes as C
 
-SPT_ABI_VERSION = 1
+SPT_ABI_VERSION = 2
+GUIDE_TRAIN_TCGEN05, GUIDE_TRAIN_MMA_SYNC = 0, 1
 SPT_MISS = 0xFFFFFFFF
 
 (SPT_OK, SPT_ERR_INVALID_ARGUMENT, SPT_ERR_CUDA, SPT_ERR_OUT_OF_MEMORY, SPT_ERR_OVERFLOW,
@@ -97,7 +98,8 @@ class BvhStats(C.Structure):
 class Tune(C.Structure):
     _fields_ = [("capacity", C.c_uint32), ("extend_block", C.c_uint32), ("shade_block", C.c_uint32),
                 ("traversal", C.c_int32), ("check_every", C.c_uint32), ("sort_shading", C.c_uint32),
-                ("reserved", C.c_uint32 * 2)]
+                ("stack", C.c_uint32), ("stack_limit", C.c_uint32), ("max_iterations", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class BatchJob(C.Structure):
@@ -107,7 +109,7 @@ class BatchJob(C.Structure):
 class GuideConfig(C.Structure):
     _fields_ = [("box_min", F3), ("box_max", F3), ("lr", C.c_float), ("batch", C.c_uint32),
                 ("max_steps", C.c_uint32), ("mix", C.c_float), ("seed", C.c_uint64),
-                ("cache_res", C.c_uint32), ("reserved", C.c_uint32)]
+                ("cache_res", C.c_uint32), ("train_path", C.c_uint32)]
 
 
 GUIDE_LEVELS, GUIDE_FEATS, GUIDE_T = 16, 2, 1 << 19

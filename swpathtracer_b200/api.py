@@ -112,6 +112,16 @@ class Bvh:
 _MODE_OUT = {abi.RAYCAST_NORMAL: (np.float32, 3), abi.RAYCAST_DEPTH: (np.float32, 1), abi.RAYCAST_COUNT: (np.int64, 1)}
 
 
+def ray_array(rays, widths):
+    """rays as a contiguous float32 [n, w] array with w in `widths`: 8 = origin, 0, direction, 0 (the
+    padded layout of spt_intersect); 6 = origin, direction (the reference's Ray, spt_intersect_packed).
+    Anything else raises ValueError: the C-ABI reads n * w floats from the pointer it is given."""
+    rays = np.ascontiguousarray(rays, np.float32)
+    if rays.ndim != 2 or rays.shape[1] not in widths:
+        raise ValueError("rays must be float32 [n, w] with w in %s, got shape %s" % (tuple(widths), rays.shape))
+    return rays
+
+
 class GpuScene:
     """A scene uploaded to the device (Scene + its acceleration structure)."""
 
@@ -148,17 +158,18 @@ class GpuScene:
         out: optional preallocated (e.g. pinned) array of abi.HIT_DTYPE for the hits; out_counts:
         optional (tests, nhits) uint32 arrays for the counts.  With every buffer page-locked, large
         batches run as a pipeline of chunks whose copies overlap the queries."""
-        rays = np.ascontiguousarray(rays, np.float32)
+        rays = ray_array(rays, (8, 6))
         n = rays.shape[0]
         hits = out if out is not None else np.zeros(n, abi.HIT_DTYPE)
-        assert hits.dtype == abi.HIT_DTYPE and hits.shape == (n,) and hits.flags["C_CONTIGUOUS"]
+        if hits.dtype != abi.HIT_DTYPE or hits.shape != (n,) or not hits.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous array of %d HIT_DTYPE records" % n)
         if out_counts is not None:
             tests, nh = out_counts
-            assert tests.dtype == np.uint32 and nh.dtype == np.uint32 and tests.shape == (n,) and nh.shape == (n,)
+            if not all(a.dtype == np.uint32 and a.shape == (n,) and a.flags["C_CONTIGUOUS"] for a in (tests, nh)):
+                raise ValueError("out_counts must be two contiguous uint32 arrays of length %d" % n)
         else:
             tests = np.zeros(n, np.uint32) if counts else None
             nh = np.zeros(n, np.uint32) if counts else None
-        assert rays.ndim == 2 and rays.shape[1] in (6, 8)
         fn = self.lib.spt_intersect_packed if rays.shape[1] == 6 else self.lib.spt_intersect
         self.dev.check(fn(self.dev.h, self.h, rays.ctypes.data, n, hits.ctypes.data,
                           None if tests is None else tests.ctypes.data, None if nh is None else nh.ctypes.data),
@@ -168,7 +179,7 @@ class GpuScene:
     def intersect_noalloc(self, rays, counts=False):
         """intersect() through spt_intersect_noalloc (include/spt_noalloc.h): no device allocation in
         the call, at most 65536 rays, calls on one device must not overlap."""
-        rays = np.ascontiguousarray(rays, np.float32)
+        rays = ray_array(rays, (8,))
         n = rays.shape[0]
         hits = np.zeros(n, abi.HIT_DTYPE)
         tests = np.zeros(n, np.uint32) if counts else None
@@ -182,6 +193,13 @@ class GpuScene:
     def intersect_device(self, d_rays, n, d_hits, stream=0):
         self.dev.check(self.lib.spt_intersect_device(self.dev.h, self.h, d_rays, n, d_hits, stream),
                        "spt_intersect_device")
+
+    def traversal_work_device(self, d_rays, n, d_hits):
+        """The closest-hit kernel's own work on n device rays: (8-wide node visits, primitive tests)."""
+        w = (C.c_uint64 * 2)()
+        self.dev.check(self.lib.spt_traversal_work_device(self.dev.h, self.h, d_rays, n, d_hits, w),
+                       "spt_traversal_work_device")
+        return int(w[0]), int(w[1])
 
     def count_device(self, d_rays, n, d_ref_hits, d_tests, d_hits, d_prim_tests=None, stream=0):
         """The reference-order traversal: its hit (d_ref_hits) and per-ray test counts; any may be None."""
@@ -261,11 +279,14 @@ def autotune(device, jobs, cache_path=None):
 
 
 def guide_config(box_min=(0, 0, 0), box_max=(1, 1, 1), lr=1e-2, batch=1 << 18, max_steps=64, mix=0.5, seed=1,
-                 cache_res=0):
+                 cache_res=0, train_path=abi.GUIDE_TRAIN_TCGEN05):
+    """train_path: abi.GUIDE_TRAIN_TCGEN05 (the training GEMMs on tcgen05 with tensor-memory
+    accumulators, tiles of 128 records) or abi.GUIDE_TRAIN_MMA_SYNC (warp-level mma.sync)."""
     c = abi.GuideConfig()
     for k in range(3):
         c.box_min[k], c.box_max[k] = box_min[k], box_max[k]
     c.lr, c.batch, c.max_steps, c.mix, c.seed, c.cache_res = lr, batch, max_steps, mix, seed, cache_res
+    c.train_path = train_path
     return c
 
 

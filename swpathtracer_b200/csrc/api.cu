@@ -1,4 +1,5 @@
 // api.cu -- context, acceleration structure and scene entry points of the C-ABI (include/spt.h).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <thread>
@@ -466,6 +467,21 @@ spt_status spt_scene_create(spt_context* ctx, const spt_scene_desc* d, const spt
             WideBvh wb;
             build_wide(tree->nodes, wb);
             wnodes.swap(wb.nodes);
+            // levels of the wide tree (breadth-first order: a node's inner children follow it), and
+            // from them the most traversal stack entries a ray can need, 2 (levels - 1)
+            std::vector<uint8_t> level(wnodes.size(), 1);
+            uint32_t levels = wnodes.empty() ? 0 : 1;
+            for (size_t k = 0; k < wnodes.size(); ++k) {
+                const uint32_t nc = static_cast<uint32_t>(__builtin_popcount(wnodes[k].imask));
+                for (uint32_t c = 0; c < nc; ++c) {
+                    const size_t ch = static_cast<size_t>(wnodes[k].child_base) + c;
+                    if (ch <= k || ch >= wnodes.size())
+                        return fail(ctx, SPT_ERR_INTERNAL, "8-wide tree is not in breadth-first order");
+                    level[ch] = static_cast<uint8_t>(std::min(255, level[k] + 1));
+                    levels = std::max<uint32_t>(levels, level[ch]);
+                }
+            }
+            sc->wide_stack_bound = levels > 1 ? 2 * (levels - 1) : 0;
             wtri.resize(3ull * wb.tri_rank.size());
             parallel_for(wb.tri_rank.size(), [&](size_t a, size_t b) {
                 for (size_t k = a; k < b; ++k) {

@@ -49,7 +49,7 @@ std::string tune_key(spt_context* ctx, const spt_batch_job* jobs, uint32_t n) {
     std::replace(name.begin(), name.end(), ' ', '_');
     char buf[64];
     std::snprintf(buf, sizeof(buf), "%016llx", static_cast<unsigned long long>(h));
-    return name + ":" + buf;
+    return "v2:" + name + ":" + buf;   // v2: entries carry the stack depth
 }
 
 bool cache_lookup(const char* path, const std::string& key, spt_tune& t) {
@@ -63,7 +63,7 @@ bool cache_lookup(const char* path, const std::string& key, spt_tune& t) {
         spt_tune c = default_tune();
         double ms;
         if (is >> k >> c.capacity >> c.extend_block >> c.shade_block >> c.traversal >> c.check_every >> c.sort_shading >>
-                ms &&
+                c.stack >> ms &&
             k == key) {
             t = c;
             found = true;  // the last entry for a key wins
@@ -76,7 +76,7 @@ void cache_store(const char* path, const std::string& key, const spt_tune& t, do
     if (!path) return;
     std::ofstream f(path, std::ios::app);
     f << key << " " << t.capacity << " " << t.extend_block << " " << t.shade_block << " " << t.traversal << " "
-      << t.check_every << " " << t.sort_shading << " " << ms << "\n";
+      << t.check_every << " " << t.sort_shading << " " << t.stack << " " << ms << "\n";
 }
 
 }  // namespace
@@ -109,8 +109,9 @@ spt_status spt_batch_pathtrace(spt_context* ctx, const spt_batch_job* jobs, uint
     return SPT_OK;
 }
 
-// Coordinate descent over the wavefront settings, each trial a render of the whole batch at 4 samples
-// per pixel into scratch images (the caller's images are not touched).
+// Coordinate descent over the wavefront settings (traversal, pool capacity, shade block, traversal
+// stack depth, grouped shading), each trial a render of the whole batch at 4 samples per pixel into
+// scratch images (the caller's images are not touched).
 spt_status spt_autotune(spt_context* ctx, const spt_batch_job* jobs, uint32_t n_jobs, const char* cache_path,
                         spt_tune* out) {
     if (!ctx || !jobs || !out || n_jobs == 0) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
@@ -152,7 +153,10 @@ spt_status spt_autotune(spt_context* ctx, const spt_batch_job* jobs, uint32_t n_
     const int32_t travs[] = {2, 1, 0};
     const uint32_t caps[] = {1u << 20, 1u << 21, 1u << 22};
     const uint32_t shades[] = {64, 128, 256};
-    const uint32_t checks[] = {4, 8, 16};
+    // stack depths that hold every scene's 8-wide tree (a shallower stack could overflow)
+    uint32_t bound = 0;
+    for (uint32_t i = 0; i < n_jobs; ++i) bound = std::max(bound, jobs[i].scene ? jobs[i].scene->wide_stack_bound : 0u);
+    const uint32_t stacks[] = {16, 24, 32};
     for (int dim = 0; dim < 5; ++dim) {
         const int n_opt = dim == 4 ? 2 : 3;
         spt_tune round_best = best;
@@ -161,7 +165,10 @@ spt_status spt_autotune(spt_context* ctx, const spt_batch_job* jobs, uint32_t n_
             if (dim == 0) c.traversal = travs[k];
             if (dim == 1) c.capacity = caps[k];
             if (dim == 2) c.shade_block = shades[k];
-            if (dim == 3) c.check_every = checks[k];
+            if (dim == 3) {
+                if (stacks[k] < bound) continue;
+                c.stack = stacks[k];
+            }
             if (dim == 4) c.sort_shading = static_cast<uint32_t>(k + 1);   // always / never
             if (std::memcmp(&c, &best, sizeof(c)) == 0) continue;
             double ms = 0.0;

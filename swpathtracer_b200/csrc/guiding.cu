@@ -467,6 +467,14 @@ size_t infer_smem_bytes() {
            kInferWarps * kTileRows * kYld * sizeof(float);
 }
 
+void k_mean_weight_launch(const float4* d_rec, uint32_t n, float* out, cudaStream_t s) {
+    k_mean_weight<<<256, 256, 0, s>>>(d_rec, n, out);
+}
+
+void k_reduce_launch(const float* partial, uint32_t chunks, uint32_t count, float* out, cudaStream_t s) {
+    k_reduce<<<(count + 255) / 256, 256, 0, s>>>(partial, chunks, count, out);
+}
+
 size_t train_smem_bytes() {
     return kSmemWeights * sizeof(__nv_bfloat16) +
            kWarps * (kTileRows * pad(kIn) + 4 * kTileRows * pad(kHid) + kTileRows * pad(kOut)) * sizeof(__nv_bfloat16) +
@@ -597,8 +605,10 @@ spt_status Guide::ensure_train_buffers(uint32_t n) {
     return SPT_OK;
 }
 
-// Gradients of the batch loss (into grid_grad / mlp_grad, which must be zero) and the loss sum.
+// Gradients of the batch loss (into grid_grad / mlp_grad, which must be zero) and the loss sum: on the
+// tensor-memory kernels (guiding_tc.cu) unless the config asks for the warp-level mma.sync kernels.
 spt_status Guide::gradients(const float4* d_rec, uint32_t n) {
+    if (cfg.train_path == SPT_GUIDE_TRAIN_TCGEN05) return gradients_tc(d_rec, n);
     spt_status st = ensure_train_buffers(n);
     if (st != SPT_OK) return st;
     cudaStream_t s = ctx->stream;
@@ -645,6 +655,7 @@ spt_status Guide::step(const float4* d_rec, uint32_t n, float* loss) {
     k_adam<<<72, 256, 0, ctx->stream>>>(mlp_master, mlp_m, mlp_v, mlp_grad, nullptr, kMlpParams, cfg.lr, c1, c2);
     k_stage<<<(kMlpParams + 255) / 256, 256, 0, ctx->stream>>>(mlp_master, smem_image);
     SPT_CUDA(ctx, cudaGetLastError());
+    if (tc_image && (st = stage_tc()) != SPT_OK) return st;
     if (loss) {
         float h[2];
         SPT_CUDA(ctx, cudaMemcpyAsync(h, scalars, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));

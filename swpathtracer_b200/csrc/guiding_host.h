@@ -11,6 +11,11 @@ namespace guide {
 
 size_t infer_smem_bytes();
 size_t train_smem_bytes();
+size_t train_tc_smem_bytes();
+size_t train_tc_image_bytes();
+// launchers of guiding.cu's helper kernels, for the tensor-memory training path (guiding_tc.cu)
+void k_mean_weight_launch(const float4* d_rec, uint32_t n, float* out, cudaStream_t s);
+void k_reduce_launch(const float* partial, uint32_t chunks, uint32_t count, float* out, cudaStream_t s);
 
 struct Guide {
     spt_context* ctx = nullptr;
@@ -29,6 +34,13 @@ struct Guide {
     float* partial = nullptr;
     uint32_t train_cap = 0;
     std::vector<void*> train_allocs;
+    // training on the tensor-memory kernels (guiding_tc.cu): the bf16 weight image in the core-matrix
+    // layout, the records' grid features, the feature gradients and one dW partial per CTA
+    unsigned char* tc_image = nullptr;
+    float* tc_partial = nullptr;
+    uint32_t* tc_feats = nullptr;
+    float* tc_dx0 = nullptr;
+    uint32_t tc_cap = 0;
     // inference scratch: the hash-grid features of up to feats_cap samples (k_encode -> k_infer)
     uint32_t* feats = nullptr;
     uint32_t feats_cap = 0;
@@ -50,8 +62,13 @@ struct Guide {
     spt_status refresh_cache();
     spt_status ensure_train_buffers(uint32_t n);
     spt_status gradients(const float4* d_rec, uint32_t n);
+    spt_status gradients_tc(const float4* d_rec, uint32_t n);
+    spt_status ensure_tc_buffers(uint32_t n);
+    spt_status stage_tc();
     spt_status step(const float4* d_rec, uint32_t n, float* loss);
     ~Guide() {
+        if (tc_feats) cudaFree(tc_feats);
+        if (tc_dx0) cudaFree(tc_dx0);
         if (feats) cudaFree(feats);
         if (cache) cudaFree(cache);
         if (cache_raw) cudaFree(cache_raw);

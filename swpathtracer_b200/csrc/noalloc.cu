@@ -18,11 +18,10 @@
 //   * the fetch counter must be zero when the kernel starts; every call clears it on its own stream
 //     before the launch.  Nothing else needs clearing: the ray area is overwritten by the upload and
 //     the hit and count areas by the kernels, for every index below n;
-//   * the first call on a device resolves the buffer's address with cudaGetSymbolAddress (with that
-//     device current), which may load the module; make that first call before any stream capture
-//     begins on the device.
-#include <mutex>
-
+//   * the first call with a context resolves the buffer's address with cudaGetSymbolAddress (with the
+//     context's device current), which may load the module; make that first call before any stream
+//     capture begins on the device.  The address is kept in the context, so a context must not be
+//     used after a cudaDeviceReset of its device (no context of this library may).
 #include "spt_internal.h"
 
 namespace spt {
@@ -44,22 +43,17 @@ static_assert(kHitsOff % 256 == 0 && kTestsOff % 256 == 0 && kPassesOff % 256 ==
 
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-void* g_address[kMaxDevices] = {};
-
-// Device address of g_scratch on the context's device (looked up once per device).
+// Device address of g_scratch on the context's device, looked up once per context (with the context's
+// device current) and kept in the context: a context lives on one device, and its lifetime ends before
+// that device's primary context could be reset under it.
 spt_status scratch_address(spt_context* ctx, unsigned char** out) {
-    if (ctx->device < 0 || ctx->device >= kMaxDevices)
-        return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "device ordinal out of range for the static buffer table");
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_address[ctx->device]) {
+    if (!ctx->noalloc_scratch) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);  // the caller made ctx->device current
         if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(static scratch)");
-        g_address[ctx->device] = p;
+        ctx->noalloc_scratch = p;
     }
-    *out = static_cast<unsigned char*>(g_address[ctx->device]);
+    *out = static_cast<unsigned char*>(ctx->noalloc_scratch);
     return SPT_OK;
 }
 

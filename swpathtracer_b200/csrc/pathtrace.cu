@@ -39,6 +39,7 @@ struct Wave {
     uint32_t n_jobs;
     uint64_t total;        // camera paths of all jobs
     uint32_t capacity;     // path slots
+    uint32_t stack_limit;  // traversal stack entries a lane may use in the persistent extend kernel
 };
 
 struct PathBuf {
@@ -173,13 +174,16 @@ __global__ void __launch_bounds__(256) k_extend(Wave W, const Counters* __restri
 }
 
 // Persistent extend: lanes take live slots from the iteration's counter as their rays finish.
+// DEPTH: the lane's traversal stack depth (tune.stack); W.stack_limit may hold it lower.
+template <int DEPTH>
 __global__ void __launch_bounds__(128) k_extend_df(Wave W, Counters* __restrict__ ctr, PathBuf cur,
                                                    float4* __restrict__ hits, uint32_t* status) {
     const Counters c = *ctr;
     const uint32_t n = c.n_alive + n_new_paths(W, c);
     const uint32_t lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    WideTraversalT<true> tr;
+    const int limit = static_cast<int>(W.stack_limit);
+    WideTraversalT<true, DEPTH> tr;
     // the lane's scene, held by value: the fields the traversal reads stay in registers instead of
     // being reloaded from the job table at every node
     DevScene S{};
@@ -213,7 +217,7 @@ __global__ void __launch_bounds__(128) k_extend_df(Wave W, Counters* __restrict_
             }
         }
         if (__all_sync(0xFFFFFFFFu, !active && exhausted)) break;
-        if (active && !tr.step(S, status)) {
+        if (active && !tr.step(S, status, limit)) {
             if (tr.finish(S)) {
                 hits[mine] = hit_record(S, tr.h);
                 active = false;
@@ -443,6 +447,18 @@ __global__ void k_advance(Wave W, Counters* ctr) {
     *ctr = c;
 }
 
+// End of one pass of the render's device-side loop (a conditional WHILE node of the CUDA graph): loop
+// again unless every path has ended, or stop with the timeout status bit once the iteration budget
+// is spent.  The budget bounds the loop whatever the kernels before it did.
+__global__ void k_continue(Wave W, const Counters* __restrict__ ctr, uint32_t max_iter, uint32_t* status,
+                           cudaGraphConditionalHandle loop) {
+    const Counters c = *ctr;
+    const bool done = c.next_path >= W.total && c.n_alive == 0;
+    const bool spent = !done && c.iterations >= max_iter;
+    if (spent) atomicOr(status, 4u);
+    cudaGraphSetConditional(loop, (done || spent) ? 0u : 1u);
+}
+
 // Training weight of every record: luminance of (radiance gathered after the record / throughput at it),
 // i.e. the path's estimate of f cos Li / p at the record.
 __global__ void k_record_weights(float4* __restrict__ rec, const float4* __restrict__ recx, uint32_t n) {
@@ -500,6 +516,7 @@ spt_status make_job(spt_context* ctx, const spt_scene* sc, const spt_camera* cam
     J.spp_offset = p->spp_offset;
     J.image = d_image;
     J.layered = sc->any_layered ? 1u : 0u;
+    J.stack_bound = sc->wide_stack_bound;
     set_sample_range(J, 0, J.spp);
     return SPT_OK;
 }
@@ -519,6 +536,9 @@ spt_tune default_tune() {
     t.shade_block = 128;
     t.traversal = -1;
     t.check_every = 8;
+    t.stack = 0;
+    t.stack_limit = 0;
+    t.max_iterations = 0;
     return t;
 }
 
@@ -531,6 +551,8 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
     if (!block_ok(tune.extend_block) || !block_ok(tune.shade_block))
         return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "tune block sizes must be multiples of 32 up to 256");
     if (tune.traversal < -1 || tune.traversal > 2) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "unknown traversal");
+    if (tune.stack != 0 && tune.stack != 16 && tune.stack != 24 && tune.stack != 32)
+        return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "tune.stack must be 0, 16, 24 or 32");
     if (train_steps) *train_steps = 0;
     uint64_t total = 0;
     int trav = 2;
@@ -609,53 +631,105 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
     }
     Counters* h_ctr;
     if ((st = pinned(ctx, sizeof(Counters), reinterpret_cast<void**>(&h_ctr))) != SPT_OK) return st;
-    Wave W{d_jobs, static_cast<uint32_t>(jobs.size()), total, static_cast<uint32_t>(cap)};
+    // traversal stack of the persistent extend kernel: the compiled depth (tune.stack, or the smallest
+    // of 16 / 24 / 32 that holds the deepest wide tree of the batch) and the entries a lane may use
+    uint32_t depth = tune.stack;
+    if (depth == 0) {
+        uint32_t need = 0;
+        for (const PtJob& J : jobs) need = std::max(need, J.stack_bound);
+        depth = need <= 16 ? 16 : need <= 24 ? 24 : 32;
+    }
+    const uint32_t limit = tune.stack_limit ? std::min(tune.stack_limit, depth) : depth;
+    Wave W{d_jobs, static_cast<uint32_t>(jobs.size()), total, static_cast<uint32_t>(cap), limit};
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
     const unsigned eb = tune.extend_block ? tune.extend_block : 128, sb = tune.shade_block ? tune.shade_block : 128;
     const unsigned g_gen = static_cast<unsigned>(std::min<uint64_t>((cap + 255) / 256, 8ull * sms));
     const unsigned g_ext = static_cast<unsigned>(std::min<uint64_t>((cap + eb - 1) / eb, 16ull * sms * 128 / eb));
     const unsigned g_shd = static_cast<unsigned>(std::min<uint64_t>((cap + sb - 1) / sb, 16ull * sms * 128 / sb));
+    auto ext_df = depth == 16 ? k_extend_df<16> : depth == 24 ? k_extend_df<24> : k_extend_df<32>;
     int per_sm = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extend_df, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ext_df, 128, 0);
     const unsigned g_df = static_cast<unsigned>(sms * std::max(1, per_sm));
-    // one CUDA graph = two iterations (A -> B, B -> A)
+    // Bound of the loop: a path lives at most ~1001 bounces (the roulette cap), plus one iteration per
+    // pool refill; tune.max_iterations may set a lower budget.
+    uint64_t max_iter = std::min<uint64_t>((total / cap + 2) * 1100ull, 0xFFFFFFF0ull);
+    if (tune.max_iterations) max_iter = std::min<uint64_t>(max_iter, tune.max_iterations);
+    // Only a guide that trains during the render needs the host between iterations (it runs the
+    // optimiser steps on the records the paths wrote).  Every other render is one launch of a graph
+    // whose WHILE node repeats two iterations until k_continue sees the pool drained.
+    const bool host_loop = guide && train_budget > 0;
+    auto record_iterations = [&](cudaGraphConditionalHandle* loop) {
+        for (int it = 0; it < 2; ++it) {
+            PathBuf& cur = it ? B : A;
+            PathBuf& nxt = it ? A : B;
+            k_generate<<<g_gen, 256, 0, ctx->stream>>>(W, d_ctr, cur);
+            if (trav == 2) ext_df<<<g_df, 128, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
+            else if (trav == 1) k_extend<1><<<g_ext, eb, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
+            else k_extend<0><<<g_ext, eb, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
+            const uint32_t* order = nullptr;
+            if (sort_shading) {
+                k_class_count<<<g_shd, 256, 0, ctx->stream>>>(W, d_ctr, cur, hits, d_class);
+                k_class_offsets<<<1, 1, 0, ctx->stream>>>(d_class, d_class + kShadeClasses);
+                k_class_scatter<<<g_shd, 256, 0, ctx->stream>>>(W, d_ctr, cur, hits, d_class + kShadeClasses, d_order);
+                order = d_order;
+            }
+            if (guide) {
+                if (train_budget > 0) k_shade<true, true><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
+                else k_shade<true, false><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
+            } else {
+                k_shade<false, false><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
+            }
+            k_advance<<<1, 1, 0, ctx->stream>>>(W, d_ctr);
+        }
+        if (loop)
+            k_continue<<<1, 1, 0, ctx->stream>>>(W, d_ctr, static_cast<uint32_t>(max_iter), ctx->d_status, *loop);
+    };
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    SPT_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    for (int it = 0; it < 2; ++it) {
-        PathBuf& cur = it ? B : A;
-        PathBuf& nxt = it ? A : B;
-        k_generate<<<g_gen, 256, 0, ctx->stream>>>(W, d_ctr, cur);
-        if (trav == 2) k_extend_df<<<g_df, 128, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
-        else if (trav == 1) k_extend<1><<<g_ext, eb, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
-        else k_extend<0><<<g_ext, eb, 0, ctx->stream>>>(W, d_ctr, cur, hits, ctx->d_status);
-        const uint32_t* order = nullptr;
-        if (sort_shading) {
-            k_class_count<<<g_shd, 256, 0, ctx->stream>>>(W, d_ctr, cur, hits, d_class);
-            k_class_offsets<<<1, 1, 0, ctx->stream>>>(d_class, d_class + kShadeClasses);
-            k_class_scatter<<<g_shd, 256, 0, ctx->stream>>>(W, d_ctr, cur, hits, d_class + kShadeClasses, d_order);
-            order = d_order;
+    cudaError_t ce = cudaSuccess;
+    if (host_loop) {
+        // one graph = two iterations (A -> B, B -> A), replayed by the host loop below
+        SPT_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        record_iterations(nullptr);
+        ce = cudaStreamEndCapture(ctx->stream, &graph);
+        if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaStreamEndCapture");
+    } else {
+        SPT_CUDA(ctx, cudaGraphCreate(&graph, 0));
+        cudaGraphConditionalHandle loop;
+        // zero-initialised in place: the C++ view of this struct has no default constructor
+        alignas(cudaGraphNodeParams) unsigned char cp_bytes[sizeof(cudaGraphNodeParams)] = {};
+        cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_bytes);
+        ce = cudaGraphConditionalHandleCreate(&loop, graph, 1u, cudaGraphCondAssignDefault);
+        if (ce == cudaSuccess) {
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = loop;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            ce = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
         }
-        if (guide) {
-            if (train_budget > 0) k_shade<true, true><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
-            else k_shade<true, false><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
-        } else {
-            k_shade<false, false><<<g_shd, sb, 0, ctx->stream>>>(W, d_ctr, cur, nxt, hits, G, order);
+        if (ce == cudaSuccess)
+            ce = cudaStreamBeginCaptureToGraph(ctx->stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal);
+        if (ce != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            return cuda_fail(ctx, ce, "building the render loop graph");
         }
-        k_advance<<<1, 1, 0, ctx->stream>>>(W, d_ctr);
+        record_iterations(&loop);
+        cudaGraph_t body = nullptr;
+        ce = cudaStreamEndCapture(ctx->stream, &body);
+        if (ce != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            return cuda_fail(ctx, ce, "cudaStreamEndCapture (render loop body)");
+        }
     }
-    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
-    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "cudaStreamEndCapture");
     ce = cudaGraphInstantiate(&exec, graph, 0);
     if (ce != cudaSuccess) {
         cudaGraphDestroy(graph);
         return cuda_fail(ctx, ce, "cudaGraphInstantiate");
     }
     SPT_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-    // Bounded loop: a path lives at most ~1001 bounces (the roulette cap), plus one iteration per pool
-    // refill; the counter check ends it as soon as all paths are done.
-    const uint64_t max_iter = (total / cap + 2) * 1100ull;
     const unsigned check = std::max(1u, tune.check_every / 2);
     uint64_t it = 0;
     bool done = false;
@@ -680,6 +754,15 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
         return SPT_OK;
     };
     st = SPT_OK;
+    if (!host_loop) {
+        // the whole render: one launch, one wait
+        ce = cudaGraphLaunch(exec, ctx->stream);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream);
+        if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+        if (ce != cudaSuccess) st = cuda_fail(ctx, ce, "path tracer render loop");
+        if (st == SPT_OK) st = check_status(ctx);   // timeout (budget spent) or stack overflow
+        done = true;
+    }
     while (!done) {
         for (unsigned k = 0; k < check; ++k, it += 2) {
             ce = cudaGraphLaunch(exec, ctx->stream);
@@ -710,7 +793,7 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
                 if ((st = train(n_rec)) != SPT_OK) break;
             }
         }
-        if (!done && it > max_iter) {
+        if (!done && it >= max_iter) {
             st = fail(ctx, SPT_ERR_TIMEOUT, "path tracer did not finish its bounded loop");
             break;
         }

@@ -51,6 +51,21 @@ __global__ void __launch_bounds__(kBlock, 10) k_intersect_df(DevScene S, const f
         });
 }
 
+// The same kernel with its own work counted (node visits, primitive tests): the work behind the
+// throughput of k_intersect_df, for comparison with the reference traversal's test counts.
+__global__ void __launch_bounds__(kBlock, 10) k_intersect_df_counted(DevScene S, const float* __restrict__ rays,
+                                                                 uint64_t n, spt_hit* __restrict__ hits,
+                                                                 uint32_t* status, unsigned long long* next,
+                                                                 unsigned long long* counts) {
+    persistent_trace<true>(
+        S, n, next, status, [&](uint64_t i, V3& o, V3& d) { load_ray<8, true>(rays, i, o, d); },
+        [&](uint64_t i, const Hit1& h) {
+            __stcs(reinterpret_cast<float4*>(hits + i),
+                   make_float4(h.t, __uint_as_float(h.found ? slot_prim(S, h.slot) : SPT_MISS), h.u, h.v));
+        },
+        counts);
+}
+
 template <int TRAV, int STRIDE>
 __global__ void __launch_bounds__(kBlock) k_intersect(DevScene S, const float* __restrict__ rays, uint64_t n,
                                                       spt_hit* __restrict__ hits, uint32_t* status) {
@@ -179,12 +194,21 @@ inline unsigned blocks_for(uint64_t n, int block) { return static_cast<unsigned>
 
 namespace {
 
-// the persistent kernel's grid (one computation per ray layout)
+// the persistent kernel's grid on the context's device (one computation per context and ray layout)
 template <int STRIDE>
 int df_grid(spt_context* ctx) {
-    static int grid = 0;
+    int& grid = ctx->df_grid[STRIDE == 6 ? 1 : 0];
     if (!grid) grid = persistent_grid(ctx, reinterpret_cast<const void*>(k_intersect_df<STRIDE>), kBlock);
     return grid;
+}
+
+// The persistent closest-hit launch.
+template <int STRIDE>
+spt_status launch_df(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
+                     unsigned long long* next, cudaStream_t s) {
+    k_intersect_df<STRIDE><<<df_grid<STRIDE>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status, next);
+    SPT_CUDA(ctx, cudaGetLastError());
+    return SPT_OK;
 }
 
 template <int STRIDE>
@@ -194,7 +218,7 @@ spt_status launch_intersect_t(spt_context* ctx, const spt_scene* sc, const float
         unsigned long long* next = nullptr;
         spt_status st = fetch_counter(ctx, s, &next);
         if (st != SPT_OK) return st;
-        k_intersect_df<STRIDE><<<df_grid<STRIDE>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status, next);
+        return launch_df<STRIDE>(ctx, sc, d_rays, n, d_hits, next, s);
     } else if (sc->dev.traversal == 1) {
         k_intersect<1, STRIDE><<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status);
     } else {
@@ -220,7 +244,19 @@ spt_status launch_intersect_fixed(spt_context* ctx, const spt_scene* sc, const f
                                   spt_hit* d_hits, unsigned long long* next, cudaStream_t s) {
     if (n == 0) return SPT_OK;
     if (sc->dev.traversal != 2) return launch_intersect(ctx, sc, d_rays, n, d_hits, s);  // no counter needed
-    k_intersect_df<8><<<df_grid<8>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status, next);
+    return launch_df<8>(ctx, sc, d_rays, n, d_hits, next, s);
+}
+
+// k_intersect_df_counted over n rays (8 floats each); counts (device): node visits, primitive tests.
+spt_status launch_intersect_counted(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n,
+                                   spt_hit* d_hits, unsigned long long* counts, cudaStream_t s) {
+    if (n == 0) return SPT_OK;
+    if (sc->dev.traversal != 2) return fail(ctx, SPT_ERR_UNSUPPORTED, "the scene has no 8-wide tree");
+    unsigned long long* next = nullptr;
+    spt_status st = fetch_counter(ctx, s, &next);
+    if (st != SPT_OK) return st;
+    static_assert(sizeof(unsigned long long) == 8, "");
+    k_intersect_df_counted<<<df_grid<8>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status, next, counts);
     SPT_CUDA(ctx, cudaGetLastError());
     return SPT_OK;
 }
@@ -368,6 +404,25 @@ spt_status spt_intersect_device(spt_context* ctx, const spt_scene* sc, const flo
                                 spt_hit* d_hits, void* stream) {
     if (!ctx || !sc || (n && (!d_rays || !d_hits))) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
     return launch_intersect(ctx, sc, d_rays, n, d_hits, static_cast<cudaStream_t>(stream));
+}
+
+spt_status spt_traversal_work_device(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n,
+                                     spt_hit* d_hits, uint64_t* work) {
+    if (!ctx || !sc || !work || (n && (!d_rays || !d_hits)))
+        return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    SPT_CUDA(ctx, cudaSetDevice(ctx->device));
+    void* d_counts;
+    spt_status st = scratch(ctx, 10, 2 * sizeof(unsigned long long), &d_counts);
+    if (st != SPT_OK) return st;
+    auto* c = static_cast<unsigned long long*>(d_counts);
+    SPT_CUDA(ctx, cudaMemsetAsync(c, 0, 2 * sizeof(unsigned long long), ctx->stream));
+    if ((st = launch_intersect_counted(ctx, sc, d_rays, n, d_hits, c, ctx->stream)) != SPT_OK) return st;
+    unsigned long long h[2] = {0, 0};
+    SPT_CUDA(ctx, cudaMemcpyAsync(h, c, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    if ((st = check_status(ctx)) != SPT_OK) return st;   // synchronises the stream
+    work[0] = h[0];
+    work[1] = h[1];
+    return SPT_OK;
 }
 
 spt_status spt_count_device(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n,

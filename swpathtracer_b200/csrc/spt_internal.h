@@ -35,6 +35,11 @@ struct spt_context {
     // ray counters of the persistent (dynamic-fetch) kernels: a ring, one slot per launch
     unsigned long long* d_fetch = nullptr;
     uint32_t fetch_slot = 0;
+    // grid of the persistent closest-hit kernel on this context's device, per ray layout (0: 8
+    // floats per ray, 1: 6), computed on first use
+    int df_grid[2] = {0, 0};
+    // device address of the static buffer of spt_intersect_noalloc (noalloc.cu), looked up on first use
+    void* noalloc_scratch = nullptr;
 };
 
 struct spt_scene {
@@ -43,6 +48,7 @@ struct spt_scene {
     std::vector<void*> allocations;
     uint64_t bytes = 0;
     uint32_t tree_height = 0;
+    uint32_t wide_stack_bound = 0;  // 2 (levels - 1) of the 8-wide tree: the most stack entries a traversal needs
     uint32_t n_materials = 0;
     bool any_emission = false;
     bool any_layered = false;      // a material with more than one BSDF layer

@@ -46,19 +46,23 @@ __device__ __forceinline__ void wide_node_hits(const DevScene& S, const WideRay&
     const float ox = (__uint_as_float(w0.x) - r.o.x) * r.ix;
     const float oy = (__uint_as_float(w0.y) - r.o.y) * r.iy;
     const float oz = (__uint_as_float(w0.z) - r.o.z) * r.iz;
-    // the near plane is the low plane when 1/d >= 0
+    // The near plane is the low plane when 1/d >= 0.  The choice is made once per node on whole
+    // words (four children's planes each), not per child and plane: 12 selects instead of 48.
     const bool nx = r.ix >= 0.0f, ny = r.iy >= 0.0f, nz = r.iz >= 0.0f;
+    const uint32_t nx0 = nx ? w2.x : w3.z, nx1 = nx ? w2.y : w3.w, fx0 = nx ? w3.z : w2.x, fx1 = nx ? w3.w : w2.y;
+    const uint32_t ny0 = ny ? w2.z : w4.x, ny1 = ny ? w2.w : w4.y, fy0 = ny ? w4.x : w2.z, fy1 = ny ? w4.y : w2.w;
+    const uint32_t nz0 = nz ? w3.x : w4.z, nz1 = nz ? w3.y : w4.w, fz0 = nz ? w4.z : w3.x, fz1 = nz ? w4.w : w3.y;
     uint32_t hits = 0, tm = 0;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         const uint32_t meta = byte_of(w1.z, w1.w, j);
         const bool inner = (imask >> j) & 1u;
-        const float lx = static_cast<float>(byte_of(w2.x, w2.y, j)), ly = static_cast<float>(byte_of(w2.z, w2.w, j));
-        const float lz = static_cast<float>(byte_of(w3.x, w3.y, j)), hx = static_cast<float>(byte_of(w3.z, w3.w, j));
-        const float hy = static_cast<float>(byte_of(w4.x, w4.y, j)), hz = static_cast<float>(byte_of(w4.z, w4.w, j));
-        const float tnx = __fmaf_rn(nx ? lx : hx, sx, ox), tfx = __fmaf_rn(nx ? hx : lx, sx, ox);
-        const float tny = __fmaf_rn(ny ? ly : hy, sy, oy), tfy = __fmaf_rn(ny ? hy : ly, sy, oy);
-        const float tnz = __fmaf_rn(nz ? lz : hz, sz, oz), tfz = __fmaf_rn(nz ? hz : lz, sz, oz);
+        const float tnx = __fmaf_rn(static_cast<float>(byte_of(nx0, nx1, j)), sx, ox);
+        const float tfx = __fmaf_rn(static_cast<float>(byte_of(fx0, fx1, j)), sx, ox);
+        const float tny = __fmaf_rn(static_cast<float>(byte_of(ny0, ny1, j)), sy, oy);
+        const float tfy = __fmaf_rn(static_cast<float>(byte_of(fy0, fy1, j)), sy, oy);
+        const float tnz = __fmaf_rn(static_cast<float>(byte_of(nz0, nz1, j)), sz, oz);
+        const float tfz = __fmaf_rn(static_cast<float>(byte_of(fz0, fz1, j)), sz, oz);
         const float tmin = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
         const float tmax = fminf(fminf(tfx, tfy), fminf(tfz, best_t));
         const bool hit = (inner || meta != 0u) && tmin <= tmax;
@@ -178,19 +182,30 @@ __device__ __forceinline__ Hit1 closest_hit_wide(const DevScene& S, V3 o, V3 d, 
 // local memory.  The path tracer's extend kernel (no register bound) gains 2-5 % from it; the
 // closest-hit kernel, held to 48 registers, would spill more and lose 9 %, so it keeps the plain
 // stack.
-template <bool REG_TOP>
+// DEPTH is the compiled stack depth (entries per lane).  A traversal needs at most one entry per wide
+// level below the root for the remaining children of an ancestor plus one per level for postponed
+// triangles, 2 (H - 1) for a wide tree of H levels; wide_stack_bound() gives that bound per scene.
+// step()'s `limit` (1 <= limit <= DEPTH) can hold a traversal to fewer entries; one that needs more
+// sets the overflow status bit instead of writing past the limit.
+// COUNT adds the lane's own work counters (node visits, primitive tests) over all of its rays.
+template <bool REG_TOP, int DEPTH = kWideStack, bool COUNT = false>
 struct WideTraversalT {
+    static_assert(DEPTH >= 1 && DEPTH <= kWideStack, "stack depth out of range");
     V3 o, d;
     WideRay r;
     Hit1 h;
-    uint2 stack[kWideStack];
+    uint2 stack[DEPTH];
     int sp;
     uint2 top;
     bool has_top;
     uint32_t g_base, g_hits, g_imask, t_base, t_mask;
     bool exact;
+    uint32_t n_nodes = 0, n_prims = 0;   // COUNT only
 
-    __device__ __forceinline__ bool can_push() const { return (REG_TOP && !has_top) || sp < kWideStack; }
+    // entries in use: the local ones plus the register top
+    __device__ __forceinline__ bool can_push(int limit) const {
+        return sp + ((REG_TOP && has_top) ? 1 : 0) < limit && sp < DEPTH;
+    }
     __device__ __forceinline__ void push(uint2 e) {
         if (!REG_TOP) {
             stack[sp++] = e;
@@ -252,10 +267,10 @@ struct WideTraversalT {
     // incoherent rays: 2,103 -> 2,568 Mrays/s.  The order of the candidates does not change the
     // result, which is the minimum over (t, rank).  A popped triangle entry is tested at the next step
     // (no node work in hand), so every entry is postponed at most once.
-    __device__ __forceinline__ bool step(const DevScene& S, uint32_t* overflow) {
+    __device__ __forceinline__ bool step(const DevScene& S, uint32_t* overflow, int limit = DEPTH) {
         const unsigned act = __activemask();
         const unsigned tri = __ballot_sync(act, t_mask != 0u);
-        if (t_mask && g_hits && can_push() && 8 * __popc(tri) < __popc(act)) {
+        if (t_mask && g_hits && can_push(limit) && 8 * __popc(tri) < __popc(act)) {
             push(make_uint2(t_base | 0x80000000u, t_mask));
             t_mask = 0;
         }
@@ -263,6 +278,7 @@ struct WideTraversalT {
             const int k = __ffs(t_mask) - 1;
             t_mask &= t_mask - 1;
             wide_candidate(S, t_base + k, o, d, h, exact);
+            if (COUNT) ++n_prims;
         }
         if (!g_hits) {
             if (empty()) return false;
@@ -281,10 +297,11 @@ struct WideTraversalT {
         const uint32_t s = key ^ r.inv_oct;
         const uint32_t child = g_base + __popc(g_imask & ((1u << s) - 1u));
         if (g_hits) {
-            if (can_push()) push(make_uint2(g_base, g_hits | (g_imask << 8)));
+            if (can_push(limit)) push(make_uint2(g_base, g_hits | (g_imask << 8)));
             else atomicOr(overflow, 1u);
         }
         wide_node_hits(S, r, child, h.t, g_base, g_hits, g_imask, t_base, t_mask);
+        if (COUNT) ++n_nodes;
         return true;
     }
 
@@ -308,12 +325,14 @@ constexpr uint32_t kChunk = 64;
 // the waiting lanes, so batching it pays a little (2,674 -> 2,690 Mrays/s at 4; 2 and 8 gain less).
 constexpr int kRefill = 4;
 
-template <typename Load, typename Store>
+// COUNT: adds the kernel's own node visits and primitive tests to counts[0] / counts[1].
+template <bool COUNT = false, typename Load, typename Store>
 __device__ __forceinline__ void persistent_trace(const DevScene& S, uint64_t n, unsigned long long* next,
-                                                 uint32_t* overflow, Load load, Store store) {
+                                                 uint32_t* overflow, Load load, Store store,
+                                                 unsigned long long* counts = nullptr) {
     const uint32_t lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
-    WideTraversalT<false> tr;
+    WideTraversalT<false, kWideStack, COUNT> tr;
     bool active = false, exhausted = false;
     uint64_t mine = 0;
     unsigned long long pool = 0, pool_end = 0;  // warp-uniform
@@ -350,6 +369,17 @@ __device__ __forceinline__ void persistent_trace(const DevScene& S, uint64_t n, 
         if (active && !tr.step(S, overflow) && tr.finish(S)) {
             store(mine, tr.h);
             active = false;
+        }
+    }
+    if (COUNT) {
+        unsigned long long a = tr.n_nodes, b = tr.n_prims;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xFFFFFFFFu, a, o);
+            b += __shfl_xor_sync(0xFFFFFFFFu, b, o);
+        }
+        if (lane == 0) {
+            atomicAdd(counts, a);
+            atomicAdd(counts + 1, b);
         }
     }
 }

@@ -21,6 +21,7 @@ struct PtJob {
     uint32_t npix;         // viewport pixels
     uint32_t spp_offset;
     uint32_t layered;      // the scene has layered materials (grouped shading pays off)
+    uint32_t stack_bound;  // traversal stack entries the scene's 8-wide tree can need (2 (levels - 1))
     uint32_t s_begin, s_end;  // the samples [s_begin, s_end) of the spp this render traces; the image is
                               // cleared when s_begin == 0 and turned into means when s_end == spp
     float* image;          // W*H*3 radiance sums, then means

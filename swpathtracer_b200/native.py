@@ -30,6 +30,7 @@ PROTOTYPES = {
     "spt_intersect_packed": (i32, [vp, vp, vp, u64, vp, vp, vp]),
     "spt_intersect_device": (i32, [vp, vp, vp, u64, vp, vp]),
     "spt_count_device": (i32, [vp, vp, vp, u64, vp, vp, vp, vp, vp]),
+    "spt_traversal_work_device": (i32, [vp, vp, vp, u64, vp, vp]),
     "spt_intersect_noalloc": (i32, [vp, vp, vp, u64, vp, vp, vp]),
     "spt_raycast_image": (i32, [vp, vp, vp, i32, vp, vp]),
     "spt_raycast_image_device": (i32, [vp, vp, vp, i32, vp, vp]),

@@ -1,16 +1,27 @@
 """Wavefront OBJ meshes for the scene front end (the reference's Scene::loadMesh, core/scene.cpp:32-68).
 
-The reference reads meshes through Assimp (aiProcess_Triangulate | aiProcess_FindDegenerates) and adds
-every triangle of every sub-mesh as a SmoothTriangle with per-corner positions and normals; a sub-mesh
-named in the script's sub_meshes list gets that material, the others get the mesh's material, or are
-skipped when render_submeshes is not "all".  Assimp is not available here; this reader follows the
-same model:
+The reference reads meshes through Assimp (aiProcess_FindDegenerates | aiProcess_Triangulate,
+core/scene.cpp:34-35; Assimp is a system package there, its version not pinned by CMakeLists.txt:30)
+and turns every three consecutive entries of a sub-mesh's vertex array into a SmoothTriangle with the
+normals at the same entries (core/scene.cpp:50-63).  Assimp's OBJ importer gives every face corner its
+own vertex, so for triangle faces those triples are the faces.  Assimp is not available here; this
+reader restates that model:
 
   * one sub-mesh per (object or group name, usemtl) run, in order of first appearance; the name is the
     current `o` / `g` name ("defaultobject" before any);
-  * polygons are split into fans (0, i, i+1);
-  * corners take their `vn` normal; a face without normals gets its geometric normal at every corner;
-  * indices may be negative (relative to the end of the list so far), `v/vt/vn`, `v//vn`, `v/vt`, `v`.
+  * polygons are split into fans (0, i, i+1), as Assimp's triangulation of a convex polygon;
+  * corners take their `vn` normal.  The reference reads mNormals for every vertex without a check
+    (core/scene.cpp:59-62), and Assimp leaves mNormals unset for a file without normals, so such a
+    face has no defined result there: it is rejected here with ValueError;
+  * degenerate faces are kept.  aiProcess_FindDegenerates, in Assimp's default configuration
+    (AI_CONFIG_PP_FD_REMOVE off), only shortens the index list of a face whose corners repeat a
+    position (turning it into a line or a point); it leaves the vertex array alone, and the
+    reference reads the vertex array, not the faces.  A face with repeated or collinear corners
+    therefore still becomes a triangle of zero area there, which the Moller-Trumbore test never hits
+    (|det| < 1e-6, primitives/triangle.cpp:20-21); the same happens here;
+  * indices may be negative (relative to the end of the list so far), `v/vt/vn`, `v//vn`; a corner
+    without a normal index (`v/vt`, `v`) is a face without normals.
+Parity with Assimp itself is unpinned: it is not present to compare with.
 """
 import numpy as np
 
@@ -63,19 +74,13 @@ def read_obj(path):
                     vi = _index(fields[0], len(verts))
                     ni = _index(fields[2], len(normals)) if len(fields) > 2 and fields[2] else None
                     corners.append((vi, ni))
+                if any(nidx is None for _, nidx in corners):
+                    raise ValueError("%s: face %r has no vertex normals; the reference reads a normal for "
+                                     "every vertex (core/scene.cpp:59-62)" % (path, line))
                 for k in range(1, len(corners) - 1):
                     tri = [corners[0], corners[k], corners[k + 1]]
-                    p = [verts[v] for v, _ in tri]
-                    if all(nidx is not None for _, nidx in tri):
-                        nrm = [normals[nidx] for _, nidx in tri]
-                    else:
-                        a, b, c3 = (np.array(x, np.float64) for x in p)
-                        g = np.cross(b - a, c3 - a)
-                        ln = np.linalg.norm(g)
-                        g = g / ln if ln > 0 else np.array([0.0, 0.0, 1.0])
-                        nrm = [list(g)] * 3
-                    current.tris.append(p)
-                    current.norms.append(nrm)
+                    current.tris.append([verts[v] for v, _ in tri])
+                    current.norms.append([normals[nidx] for _, nidx in tri])
     return [meshes[k] for k in order]
 
 

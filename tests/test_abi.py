@@ -103,3 +103,61 @@ def test_handles_are_freed_once_and_before_their_context():
     b.release()                      # a late close of the guide is a no-op
     d.close()
     assert calls == [("scene", 10), ("guide", 20), ("ctx", 1)]
+
+
+def _corrupt(packed, **arrays):
+    """A copy of packed's description with some arrays replaced (kept alive on the returned object)."""
+    d = abi.SceneDesc.from_buffer_copy(packed.desc)
+
+    class Keep:
+        pass
+    k = Keep()
+    k.desc = d
+    for name, a in arrays.items():
+        setattr(k, name, a)
+        if name == "mats":
+            d.prim_material = abi.ptr(a, C.c_uint32)
+        elif name == "types":
+            d.prim_type = abi.ptr(a, C.c_uint8)
+        elif name == "layered_ids":
+            d.layered_bsdf_ids = abi.ptr(a, C.c_uint32)
+        elif name == "layered_offsets":
+            d.layered_offsets = abi.ptr(a, C.c_uint32)
+    return k
+
+
+def test_corrupt_scene_tables_are_rejected():
+    """Tables that point outside themselves are caught by the scene validation before any build or
+    upload (spt_bvh_build runs it on the host, spt_scene_create and spt_bvh_build_device the same)."""
+    L = native.lib()
+    packed = scenes.box_scene(1).build()
+    h = C.c_void_p()
+    bad_mat = packed.mats.copy()
+    bad_mat[3] = packed.n_materials                       # material index out of range
+    bad_type = packed.types.copy()
+    bad_type[0] = 7                                       # unknown primitive type
+    bad_ids = packed.layered_ids.copy()
+    bad_ids[0] = 1000                                     # layered stack names a missing BSDF
+    bad_offs = packed.layered_offsets.copy()
+    bad_offs[1] = bad_offs[0]                             # a layered stack with no layer
+    for k in (_corrupt(packed, mats=bad_mat), _corrupt(packed, types=bad_type),
+              _corrupt(packed, layered_ids=bad_ids), _corrupt(packed, layered_offsets=bad_offs)):
+        assert L.spt_bvh_build(C.byref(k.desc), 1, C.byref(h)) == abi.SPT_ERR_INVALID_ARGUMENT
+    orig = packed.bsdfs[0].type
+    packed.bsdfs[0].type = 99                             # unknown BSDF type
+    try:
+        assert L.spt_bvh_build(packed.ref(), 1, C.byref(h)) == abi.SPT_ERR_INVALID_ARGUMENT
+    finally:
+        packed.bsdfs[0].type = orig
+    assert L.spt_bvh_build(packed.ref(), 1, C.byref(h)) == abi.SPT_OK
+    L.spt_bvh_free(h)
+
+
+def test_ray_arrays_of_the_wrong_shape_are_rejected():
+    from swpathtracer_b200.api import ray_array
+    r = scenes.incoherent_rays(10, seed=1)
+    assert ray_array(r, (8,)).shape == (10, 8)
+    assert ray_array(r[:, :6], (8, 6)).shape == (10, 6)
+    for bad, widths in ((r[:, :6], (8,)), (r[:, :7], (8, 6)), (r[:, 0], (8, 6))):
+        with pytest.raises(ValueError):
+            ray_array(bad, widths)

@@ -1,5 +1,6 @@
 """The guiding model on the GPU against its CPU restatement (oracle/guiding_ref.py): forward pass
-(bf16 tensor-core MLP), gradients of the loss (MLP weights and hash grid) and the Adam step."""
+(bf16 tensor-core MLP), gradients of the loss (MLP weights and hash grid) on both training paths and
+the Adam step."""
 import numpy as np
 import pytest
 
@@ -23,8 +24,8 @@ def _mlp_list(flat):
     return out
 
 
-def _guide(device, seed=3):
-    g = spt.Guide(device, spt.guide_config(seed=seed))
+def _guide(device, seed=3, train_path=abi.GUIDE_TRAIN_TCGEN05):
+    g = spt.Guide(device, spt.guide_config(seed=seed, train_path=train_path))
     grid, mlp = g.get_params()
     rng = np.random.default_rng(seed)
     grid = rng.uniform(-0.5, 0.5, grid.shape).astype(np.float32)   # non-trivial features
@@ -65,10 +66,14 @@ def test_forward_matches_oracle(device):
     g.close()
 
 
-def test_gradients_match_oracle(device):
-    g, grid, mlp = _guide(device, seed=4)
+@pytest.mark.parametrize("path,n", [(abi.GUIDE_TRAIN_TCGEN05, 4000), (abi.GUIDE_TRAIN_MMA_SYNC, 4000),
+                                    (abi.GUIDE_TRAIN_TCGEN05, 1 << 18), (abi.GUIDE_TRAIN_TCGEN05, 77)])
+def test_gradients_match_oracle(device, path, n):
+    """Both training paths (tcgen05 tiles of 128 records with tensor-memory accumulators, and the
+    warp-level mma.sync kernels), at the configured batch of 2^18 records, a ragged batch and one
+    smaller than a tile."""
+    g, grid, mlp = _guide(device, seed=4, train_path=path)
     rng = np.random.default_rng(6)
-    n = 4000
     recs = _records(rng, n)
     ggrid, gmlp, loss = g.gradients(recs)
     y, xs, corners = _oracle_outputs(grid, mlp, recs["pos"], recs["normal"], recs["wo"])

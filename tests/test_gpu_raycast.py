@@ -92,8 +92,9 @@ def test_empty_and_ragged_batches(device, oracle):
 
 def test_full_size_mesh_closest_equals_exhaustive(device):
     """1,310,720 triangles, 2^24 incoherent rays: the ordered, pruned traversal returns exactly the
-    hit of the reference-order exhaustive traversal for every ray (size-independent property), and a
-    sample agrees with the oracle."""
+    hit of the reference-order exhaustive traversal for every ray (a size-independent property of
+    the two GPU kernels).  The comparison of a sample of the same rays with the reference's own
+    hits is test_gpu_config_pins.py::test_c1_headline_rays_match_reference."""
     import torch
     packed = scenes.displaced_mesh_scene(8).build()
     gs = spt.GpuScene(device, packed)

@@ -10,7 +10,7 @@ import pytest
 from swpathtracer_b200 import abi, frontend, lua, obj
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference"
+REF = os.environ.get("SPT_REFERENCE_DIR", "/root/reference")
 
 
 def run(src, **globals_):
@@ -128,15 +128,15 @@ def test_front_end_builds_the_test_scene():
 
 def test_obj_reader(tmp_path):
     p = tmp_path / "m.obj"
-    p.write_text("v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nvn 0 0 1\n"
+    p.write_text("v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nvn 0 0 1\nvn 0 1 0\n"
                  "o first\nf 1//1 2//1 3//1 4//1\n"          # a quad with normals -> 2 triangles
-                 "g second\nusemtl red\nf -4 -3 -2\n"          # relative indices, no normals
-                 "usemtl blue\nf 1/1 3/1 4/1\n")
+                 "g second\nusemtl red\nf -4//-1 -3//-1 -2//-2\n"   # relative indices
+                 "usemtl blue\nf 1/1/1 3/1/2 4/1/1\n")
     meshes = obj.read_obj(str(p))
     assert [m.name for m in meshes] == ["first", "second", "second"]
     assert [len(m.tris) for m in meshes] == [2, 1, 1]
     np.testing.assert_allclose(meshes[0].tris[1], [[0, 0, 0], [1, 1, 0], [0, 1, 0]])
-    np.testing.assert_allclose(meshes[1].norms[0], [[0, 0, 1]] * 3)
+    np.testing.assert_allclose(meshes[1].norms[0], [[0, 1, 0], [0, 1, 0], [0, 0, 1]])
     from swpathtracer_b200 import scenes
     sb = scenes.SceneBuilder()
     m0 = sb.material(sb.layered_bsdf(sb.lambertian()))
@@ -157,3 +157,40 @@ def test_reference_samples_load(name, prims, integrator):
     assert s.packed.n_prims == prims
     assert s.integrator == integrator
     assert s.camera.width > 0 and s.pt_params.spp > 0
+
+
+def test_obj_without_normals_is_rejected(tmp_path):
+    """The reference reads mNormals for every vertex (core/scene.cpp:59-62); a file without normals
+    has no defined result there, so the reader refuses it instead of inventing normals."""
+    p = tmp_path / "n.obj"
+    p.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\n")
+    with pytest.raises(ValueError):
+        obj.read_obj(str(p))
+    p.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nvn 0 0 1\nf 1//1 2//1 3\n")   # one corner without
+    with pytest.raises(ValueError):
+        obj.read_obj(str(p))
+
+
+def test_obj_degenerate_faces_are_kept_and_never_hit(tmp_path, oracle):
+    """aiProcess_FindDegenerates (default configuration) leaves the vertex array the reference reads
+    untouched, so faces with a repeated corner or collinear corners still become triangles; their
+    zero area makes the Moller-Trumbore test reject every ray (primitives/triangle.cpp:20-21)."""
+    from swpathtracer_b200 import scenes
+    p = tmp_path / "d.obj"
+    p.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nv 2 0 0\nvn 0 0 1\n"
+                 "f 1//1 2//1 3//1\n"        # a proper triangle
+                 "f 1//1 2//1 2//1\n"        # a repeated corner
+                 "f 1//1 2//1 4//1\n")       # three collinear corners
+    meshes = obj.read_obj(str(p))
+    assert [len(m.tris) for m in meshes] == [3]
+    sb = scenes.SceneBuilder()
+    m = sb.material(sb.layered_bsdf(sb.lambertian()))
+    assert obj.add_mesh(sb, str(p), m) == 3
+    packed = sb.build()
+    rays = np.zeros((3, 8), np.float32)
+    rays[:, 0:3] = [[0.2, 0.2, 1.0], [0.5, 0.0, 1.0], [1.5, 0.0, 1.0]]   # onto the proper triangle and
+    rays[:, 4:7] = [0.0, 0.0, -1.0]                                      # onto the two degenerate ones
+    r = oracle.scene(packed).intersect(rays)
+    assert list(r["hits"]["prim_id"][:1]) == [0]
+    assert r["hits"]["prim_id"][2] == abi.SPT_MISS      # only the collinear face spans x = 1.5
+    assert r["hits"]["prim_id"][1] in (0, abi.SPT_MISS)  # x = 0.5, y = 0 lies on the proper triangle's edge
