@@ -47,6 +47,8 @@ def args_():
     p.add_argument("--c4-spp", type=int, default=256)
     p.add_argument("--c4-ref-spp", type=int, default=4096)
     p.add_argument("--c4-steps", type=int, default=32)
+    p.add_argument("--guide-train-only", action="store_true",
+                   help="only the guide's training-step times on 2^18 device records (one JSON line)")
     return p.parse_args()
 
 
@@ -294,6 +296,33 @@ def guided_c4(spt, scenes, dev, torch, spp=256, ref_spp=4096, batch=1 << 18, ste
     return out
 
 
+def guide_train_steps(spt, abi, dev, torch, n=1 << 18, steps=10, warmup=3):
+    """Device time of one optimiser step of the guide on n records already in device memory
+    (spt_guide_train_device), for both training paths: tcgen05 tiles of 128 records with tensor-memory
+    accumulators, and the warp-level mma.sync kernels.  Synthetic records: positions uniform in the
+    unit box, directions uniform on the sphere, weights uniform in [0, 2)."""
+    import numpy as np
+    rng = np.random.default_rng(1)
+    r = np.zeros(n, abi.GUIDE_RECORD_DTYPE)
+    r["pos"] = rng.uniform(0.02, 0.98, (n, 3))
+    for k in ("normal", "wo", "wi"):
+        v = rng.normal(size=(n, 3))
+        r[k] = v / np.linalg.norm(v, axis=1, keepdims=True)
+    r["weight"] = rng.uniform(0.0, 2.0, n)
+    d = torch.from_numpy(r.view(np.uint8).copy()).cuda()
+    out = {}
+    for name, path in (("tcgen05", abi.GUIDE_TRAIN_TCGEN05), ("mma_sync", abi.GUIDE_TRAIN_MMA_SYNC)):
+        g = spt.Guide(dev, spt.guide_config(batch=n, train_path=path, seed=2))
+        for _ in range(warmup):
+            g.train_device(d.data_ptr(), n)
+        ms = sorted(g.train_device(d.data_ptr(), n) for _ in range(steps))
+        g.close()
+        med = ms[len(ms) // 2]
+        out["guide_train_step_2e18_%s_ms" % name] = round(med, 4)
+        out["guide_train_step_2e18_%s_Mrecords_s" % name] = round(n / (med / 1e3) / 1e6, 1)
+    return out
+
+
 def cpu_pathtrace_baseline(subdiv):
     """The reference's own PathTracer::render (oracle/_ref) on this host's cores, on bounded samples of
     the two path-tracing workloads (4 spp of the box scene, 1 spp of the layered 1.3M-tri scene).
@@ -373,6 +402,11 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    if a.guide_train_only:
+        dev = spt.Device(local)
+        print(json.dumps(guide_train_steps(spt, abi, dev, torch)), flush=True)
+        dev.close()
+        return
     if a.c4_only:
         dev = spt.Device(local)
         print(json.dumps(guided_c4(spt, scenes, dev, torch, spp=a.c4_spp, ref_spp=a.c4_ref_spp, steps=a.c4_steps)),
@@ -578,6 +612,8 @@ def main():
                                       scenes.small_light_box_scene(), 4096, 16384, 32, seeds=(7,)))
         # guided rendering on a sample of the batch set (box with a 0.25 x 0.25 ceiling light)
         extras.update(guided_batch_sample(spt, scenes, dev, torch))
+        # the guide's optimiser step at the configured batch of 2^18 records
+        extras.update(guide_train_steps(spt, abi, dev, torch))
         out["submetrics"] = extras
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(packed, rays_np, 1 << 22)

@@ -306,7 +306,9 @@ typedef struct spt_guide_config {
     float box_min[3], box_max[3];  /* positions are normalised by this box (e.g. the scene bounds) */
     float lr;                      /* Adam learning rate */
     uint32_t batch;                /* training records per optimiser step */
-    uint32_t max_steps;            /* optimiser steps per guided render before the model is frozen */
+    uint32_t max_steps;            /* optimiser steps per guided render before the model is frozen: a
+                                      render takes one step per 10 batches of its camera paths, at
+                                      least one, at most max_steps (0: the guide stays frozen) */
     float mix;                     /* probability of sampling the guiding distribution */
     uint64_t seed;                 /* parameter initialisation */
     uint32_t cache_res;            /* cells per axis of the lobe cache guided renders sample: 4..64, 0 = 32 */
@@ -340,11 +342,16 @@ spt_status spt_guide_gradients(spt_context* ctx, spt_guide* guide, const spt_gui
                                float* grid_grad, float* mlp_grad, float* loss);
 /* One Adam step on n records (host). */
 spt_status spt_guide_train(spt_context* ctx, spt_guide* guide, const spt_guide_record* recs, uint32_t n, float* loss);
+/* One Adam step on n records already in device memory (the spt_guide_record layout, 64 bytes each);
+ * gpu_ms (may be NULL): the step's device time.  Returns after the step has finished. */
+spt_status spt_guide_train_device(spt_context* ctx, spt_guide* guide, const spt_guide_record* d_recs, uint32_t n,
+                                  float* gpu_ms);
 /* Optimiser steps taken by the guide since it was created. */
 spt_status spt_guide_steps(spt_guide* guide, uint64_t* steps);
-/* Guided path tracing: as spt_pathtrace_device, sampling guidable vertices (single-layer Lambertian /
- * Cook-Torrance) from mix * guide + (1 - mix) * BSDF, and training the guide on its own paths for up to
- * cfg.max_steps steps. */
+/* Guided path tracing: as spt_pathtrace_device, sampling guidable vertices from mix * guide +
+ * (1 - mix) * BSDF (single-layer Lambertian / Cook-Torrance; a smooth dielectric over Cook-Torrance
+ * through its walk's single-internal-bounce component), and training the guide on its own paths (the
+ * step budget of spt_guide_config.max_steps). */
 spt_status spt_guided_pathtrace_device(spt_context* ctx, const spt_scene* scene, const spt_camera* cam,
                                        const spt_pt_params* params, spt_guide* guide, float* d_out_rgb,
                                        spt_render_stats* stats);

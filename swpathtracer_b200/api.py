@@ -350,6 +350,14 @@ class Guide:
                                                     mlp.ctypes.data, C.byref(loss)), "spt_guide_gradients")
         return grid, mlp, loss.value
 
+    def train_device(self, d_recs, n):
+        """One Adam step on n records already on the device (d_recs: device pointer to n
+        GUIDE_RECORD_DTYPE records); returns the step's device time in ms."""
+        ms = C.c_float()
+        self.dev.check(self.lib.spt_guide_train_device(self.dev.h, self.h, d_recs, n, C.byref(ms)),
+                       "spt_guide_train_device")
+        return ms.value
+
     def train(self, recs):
         recs = np.ascontiguousarray(recs, abi.GUIDE_RECORD_DTYPE)
         loss = C.c_float()

@@ -122,6 +122,20 @@ spt_status spt_guide_train(spt_context* ctx, spt_guide* guide, const spt_guide_r
     return check_status(ctx);
 }
 
+spt_status spt_guide_train_device(spt_context* ctx, spt_guide* guide, const spt_guide_record* d_recs, uint32_t n,
+                                  float* gpu_ms) {
+    if (!ctx || !guide || !d_recs || n == 0) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (guide->g.ctx != ctx) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "the guide belongs to another context");
+    SPT_CUDA(ctx, cudaSetDevice(ctx->device));
+    SPT_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+    spt_status st = guide->g.step(reinterpret_cast<const float4*>(d_recs), n, nullptr);
+    if (st != SPT_OK) return st;
+    SPT_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+    if ((st = check_status(ctx)) != SPT_OK) return st;   // synchronises the stream
+    if (gpu_ms) SPT_CUDA(ctx, cudaEventElapsedTime(gpu_ms, ctx->ev0, ctx->ev1));
+    return SPT_OK;
+}
+
 spt_status spt_guide_steps(spt_guide* guide, uint64_t* steps) {
     if (!guide || !steps) return SPT_ERR_INVALID_ARGUMENT;
     *steps = guide->g.steps;
@@ -142,7 +156,12 @@ spt_status spt_guided_pathtrace_device(spt_context* ctx, const spt_scene* sc, co
     // mean of all samples) is too.
     const PtJob whole = jobs[0];
     const uint32_t spp = whole.spp, npix = std::max(1u, whole.npix);
-    const uint32_t budget = guide->g.cfg.max_steps;
+    // Training is paid for out of the render's own time, so its step budget grows with the render:
+    // one optimiser step per 10 batches' worth of camera paths (about a fifth of a plain render's
+    // time at 2^18 records per step), at least one and at most max_steps.
+    const uint64_t per_step = 10ull * std::max(1u, guide->g.cfg.batch);
+    const uint32_t budget = static_cast<uint32_t>(
+        std::min<uint64_t>(guide->g.cfg.max_steps, std::max<uint64_t>(1, whole.total / per_step)));
     uint32_t pass = std::max(1u, (guide->g.cfg.batch + npix - 1) / npix);
     uint64_t segs = 0, paths = 0;
     double ms = 0.0;

@@ -343,12 +343,14 @@ __global__ void __launch_bounds__(kTcRows, 1) k_train_tc(TcIO io) {
                     }
                     put16(dz, tid, 8u * c, kHid, make_uint4(o[0], o[1], o[2], o[3]));
                 }
-            } else if (valid) {
+            } else {
                 float v[kIn];
-                ld_row<kIn>(tmem, 0, v);
-                float4* dst = reinterpret_cast<float4*>(io.dx0 + 32ull * row);
+                ld_row<kIn>(tmem, 0, v);   // every lane of the warp takes part in the load
+                if (valid) {
+                    float4* dst = reinterpret_cast<float4*>(io.dx0 + 32ull * row);
 #pragma unroll
-                for (int c = 0; c < 8; ++c) dst[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+                    for (int c = 0; c < 8; ++c) dst[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+                }
             }
             tc::fence_proxy_async();
             tc::fence_before_sync();

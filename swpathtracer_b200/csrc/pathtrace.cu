@@ -347,26 +347,35 @@ __global__ void __launch_bounds__(256, 3) k_shade(Wave W, Counters* __restrict__
                 Stream bs(J.seed, path, static_cast<uint32_t>(depth) + 1u);
                 V3 f, refl, wi, wwi;
                 float pdf;
-                const uint32_t gi = (GUIDED && guidable(J.S, m)) ? cache_cell(G, pos, nrm) : kNoRec;
-                if (GUIDED && gi != kNoRec) {
-                    const GuidedSample gs =
-                        guided_sample(J.S, m, frame, wo, G.cache + static_cast<uint64_t>(guide::kCacheEntry) * gi, G.mix, bs);
+                // guided: single-layer materials (guided_sample), and the coated stack from outside
+                // (its walk below is the second technique)
+                const bool coat = GUIDED && coated(J.S, m);
+                const uint32_t gi =
+                    (GUIDED && guidable(J.S, m) && (!coat || wo.y > 0.0f)) ? cache_cell(G, pos, nrm) : kNoRec;
+                const float* entry = G.cache + static_cast<uint64_t>(guide::kCacheEntry) * (gi != kNoRec ? gi : 0u);
+                bool sampled = false;
+                if (GUIDED && gi != kNoRec && (!coat || bs.next() < G.mix)) {
+                    const GuidedSample gs = coat ? coated_guide_sample(J.S, m, frame, wo, entry, G.mix, bs)
+                                                 : guided_sample(J.S, m, frame, wo, entry, G.mix, bs);
                     f = gs.f;
                     refl = gs.refl;
                     wi = gs.wi_local;
                     wwi = gs.wi_world;
                     pdf = gs.p;
-                    if (!(pdf > 0.0f)) {
-                        f = v3(0.0f, 0.0f, 0.0f);
-                        pdf = 1.0f;
-                    }
-                } else {
+                    sampled = true;
+                }
+                if (!sampled) {
                     const LayerEval e = eval_layered(J.S, m, wo, bs);
                     f = e.f;
                     refl = e.refl;
                     wi = e.wi;
                     pdf = e.pdf;
                     wwi = mat_mul(frame, e.wi);                    // pathtracer.cpp:37-38
+                    if (GUIDED && gi != kNoRec) coated_walk_weight(J.S, m, wo, wwi, e, entry, G.mix, f, pdf);
+                }
+                if (GUIDED && gi != kNoRec && !(pdf > 0.0f)) {
+                    f = v3(0.0f, 0.0f, 0.0f);
+                    pdf = 1.0f;
                 }
                 const V3 no = pos + wwi * 1e-3f;
                 const V3 le = v3(m.er, m.eg, m.eb);

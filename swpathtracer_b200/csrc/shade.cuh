@@ -171,6 +171,8 @@ __device__ __forceinline__ V3 bsdf_refl(const DevBsdf& b, V3 wo, V3 wi) {
 struct LayerEval {
     V3 f, refl, wi;
     float pdf;
+    int bounces;    // layer events of the walk
+    bool out_top;   // the walk left through the top of the stack
 };
 
 // LayeredBSDF::evalBSDF (materials/layered_bsdf.cpp:10-74): random walk through the layer stack,
@@ -209,6 +211,8 @@ __device__ __forceinline__ LayerEval eval_layered(const DevScene& S, const DevMa
     }
     LayerEval r;
     r.wi = wi;
+    r.bounces = bounce;
+    r.out_top = id == -1;
     if ((bounce < 500) && !inf && (fp > 0.0f)) {
         r.pdf = fp;
         r.f = fb;

@@ -215,13 +215,16 @@ struct WideTraversalT {
         top = e;
         has_top = true;
     }
-    __device__ __forceinline__ bool empty() const { return !(REG_TOP && has_top) && sp == 0; }
+    // With REG_TOP the register entry is the stack's top whenever the stack is not empty: a pop
+    // returns it and at once loads the next entry from local memory into the register, so that load
+    // has the whole next node visit to arrive before the following pop needs it.
+    __device__ __forceinline__ bool empty() const { return REG_TOP ? !has_top : sp == 0; }
     __device__ __forceinline__ uint2 pop() {
-        if (REG_TOP && has_top) {
-            has_top = false;
-            return top;
-        }
-        return stack[--sp];
+        if (!REG_TOP) return stack[--sp];
+        const uint2 r = top;
+        if (sp > 0) top = stack[--sp];
+        else has_top = false;
+        return r;
     }
 
     // Returns false when the ray is already finished (empty scene or root box missed).  The root node

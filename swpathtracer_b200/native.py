@@ -52,6 +52,7 @@ PROTOTYPES = {
     "spt_guide_eval": (i32, [vp, vp, vp, u32, vp]),
     "spt_guide_gradients": (i32, [vp, vp, vp, u32, vp, vp, vp]),
     "spt_guide_train": (i32, [vp, vp, vp, u32, vp]),
+    "spt_guide_train_device": (i32, [vp, vp, vp, u32, C.POINTER(C.c_float)]),
     "spt_guide_steps": (i32, [vp, C.POINTER(C.c_uint64)]),
     "spt_guided_pathtrace_device": (i32, [vp, vp, vp, vp, vp, vp, vp]),
 }
