@@ -316,6 +316,9 @@ typedef struct spt_guide_config {
                                       tensor cores, tiles of 128 records with fp32 accumulators in tensor
                                       memory; SPT_GUIDE_TRAIN_MMA_SYNC (1): warp-level mma.sync tiles of
                                       32 records */
+    uint32_t guided_depth;         /* vertices guided per path: those at depth < guided_depth (the camera
+                                      ray's hit is depth 0); 0 = every vertex */
+    uint32_t reserved;             /* must be 0 */
 } spt_guide_config;
 
 /* One training record: a scattering event and the radiance it led to. */

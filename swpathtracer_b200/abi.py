@@ -109,7 +109,8 @@ class BatchJob(C.Structure):
 class GuideConfig(C.Structure):
     _fields_ = [("box_min", F3), ("box_max", F3), ("lr", C.c_float), ("batch", C.c_uint32),
                 ("max_steps", C.c_uint32), ("mix", C.c_float), ("seed", C.c_uint64),
-                ("cache_res", C.c_uint32), ("train_path", C.c_uint32)]
+                ("cache_res", C.c_uint32), ("train_path", C.c_uint32), ("guided_depth", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 GUIDE_LEVELS, GUIDE_FEATS, GUIDE_T = 16, 2, 1 << 19

@@ -279,14 +279,15 @@ def autotune(device, jobs, cache_path=None):
 
 
 def guide_config(box_min=(0, 0, 0), box_max=(1, 1, 1), lr=1e-2, batch=1 << 18, max_steps=64, mix=0.5, seed=1,
-                 cache_res=0, train_path=abi.GUIDE_TRAIN_TCGEN05):
+                 cache_res=0, train_path=abi.GUIDE_TRAIN_TCGEN05, guided_depth=0):
     """train_path: abi.GUIDE_TRAIN_TCGEN05 (the training GEMMs on tcgen05 with tensor-memory
-    accumulators, tiles of 128 records) or abi.GUIDE_TRAIN_MMA_SYNC (warp-level mma.sync)."""
+    accumulators, tiles of 128 records) or abi.GUIDE_TRAIN_MMA_SYNC (warp-level mma.sync).
+    guided_depth: guide the path vertices at depth < guided_depth only (0: all)."""
     c = abi.GuideConfig()
     for k in range(3):
         c.box_min[k], c.box_max[k] = box_min[k], box_max[k]
     c.lr, c.batch, c.max_steps, c.mix, c.seed, c.cache_res = lr, batch, max_steps, mix, seed, cache_res
-    c.train_path = train_path
+    c.train_path, c.guided_depth = train_path, guided_depth
     return c
 
 

@@ -44,9 +44,19 @@ __device__ __forceinline__ float sampler_density(const DevBsdf& b, V3 wo, V3 wi)
     const float nh = h.y;
     if (!(nh > 0.0f)) return 0.0f;
     const float m2 = b.scalar * b.scalar, nh2 = nh * nh;
-    const float d = expf((nh2 - 1.0f) / (m2 * nh2)) / (kPi * m2 * nh2 * nh2);
+    // where the Beckmann exponential underflows the density is 0 (the 1 / nh^4 factor alone would
+    // overflow and turn the product into NaN)
+    const float e = expf((nh2 - 1.0f) / (m2 * nh2));
+    if (!(e > 0.0f)) return 0.0f;
+    const float d = e / (kPi * m2 * nh2 * nh2);
     const float om = fabsf(dot(wi, h));
     return om > 0.0f ? d * nh / (4.0f * om) : 0.0f;
+}
+
+// A BSDF value at a direction the guide chose.  Far outside a narrow Cook-Torrance lobe the reference's
+// f (bsdf_f, kept bit for bit) meets 0 * infinity; its limit there is 0.
+__device__ __forceinline__ V3 finite_or_zero(V3 f) {
+    return (isfinite(f.x) && isfinite(f.y) && isfinite(f.z)) ? f : v3(0.0f, 0.0f, 0.0f);
 }
 
 struct GuidedSample {
@@ -87,7 +97,7 @@ __device__ __forceinline__ CoatT1 coat_t1(const DevBsdf& top, const DevBsdf& bot
     const float pct = sampler_density(bot, wop, wip);
     if (!(pct > 0.0f)) return r;
     const float k = t / (eta * eta);
-    r.f = bsdf_f(bot, wop, wip) * k;
+    r.f = finite_or_zero(bsdf_f(bot, wop, wip)) * k;
     r.p = k * pct * w.y / wip.y;
     r.refl = bsdf_refl(bot, wop, wip);
     return r;
@@ -144,7 +154,7 @@ __device__ __forceinline__ GuidedSample guided_sample(const DevScene& S, const D
         g.wi_world = mat_mul(frame, bs.wi);
     }
     const V3 wi = g.wi_local;
-    g.f = wi.y > 0.0f ? bsdf_f(b, wo, wi) : v3(0.0f, 0.0f, 0.0f);
+    g.f = wi.y > 0.0f ? finite_or_zero(bsdf_f(b, wo, wi)) : v3(0.0f, 0.0f, 0.0f);
     g.refl = wi.y > 0.0f ? bsdf_refl(b, wo, wi) : v3(0.0f, 0.0f, 0.0f);
     g.p = mix * guide::cached_mixture_pdf(entry, g.wi_world) + (1.0f - mix) * sampler_density(b, wo, wi);
     return g;

@@ -69,6 +69,7 @@ struct Counters {
 struct GuideIO {
     float mix;
     uint32_t rec_cap;
+    uint32_t depth;        // vertices at path depth < depth are guided
     const float* cache;    // the guide's mixture per (position cell, normal axis): guide::kCacheEntry floats each
     uint32_t cache_res;    // cells per axis over the guide's box
     float lo[3], inv_ext[3];
@@ -350,8 +351,10 @@ __global__ void __launch_bounds__(256, 3) k_shade(Wave W, Counters* __restrict__
                 // guided: single-layer materials (guided_sample), and the coated stack from outside
                 // (its walk below is the second technique)
                 const bool coat = GUIDED && coated(J.S, m);
-                const uint32_t gi =
-                    (GUIDED && guidable(J.S, m) && (!coat || wo.y > 0.0f)) ? cache_cell(G, pos, nrm) : kNoRec;
+                const uint32_t gi = (GUIDED && static_cast<uint32_t>(depth) < G.depth && guidable(J.S, m) &&
+                                     (!coat || wo.y > 0.0f))
+                                        ? cache_cell(G, pos, nrm)
+                                        : kNoRec;
                 const float* entry = G.cache + static_cast<uint64_t>(guide::kCacheEntry) * (gi != kNoRec ? gi : 0u);
                 bool sampled = false;
                 if (GUIDED && gi != kNoRec && (!coat || bs.next() < G.mix)) {
@@ -627,6 +630,7 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
         G.recx = G.rec + 4ull * rec_cap;
         G.mix = guide->cfg.mix;
         G.rec_cap = rec_cap;
+        G.depth = guide->cfg.guided_depth ? guide->cfg.guided_depth : 0xFFFFFFFFu;
         if ((st = guide->refresh_cache()) != SPT_OK) return st;
         G.cache = guide->cache;
         G.cache_res = guide->cache_res;

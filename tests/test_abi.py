@@ -43,7 +43,7 @@ def test_struct_sizes_match_header():
     assert C.sizeof(abi.Bvh2Node) == 32 and abi.BVH2_NODE_DTYPE.itemsize == 32
     assert C.sizeof(abi.PtParams) == 32
     assert C.sizeof(abi.Camera) == 84
-    assert C.sizeof(abi.GuideConfig) == 56
+    assert C.sizeof(abi.GuideConfig) == 64
 
 
 def test_bvh_build_rejects_bad_descriptions():

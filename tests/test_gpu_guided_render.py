@@ -103,7 +103,8 @@ def test_guided_window_room_is_unbiased_and_less_noisy(device, mix):
 
 
 def test_guided_equals_plain_without_guidable_materials(device):
-    gs = spt.GpuScene(device, scenes.furnace_scene("coating").build())
+    # a dielectric over a Lambertian layer: a stack guiding leaves to the reference's walk
+    gs = spt.GpuScene(device, scenes.furnace_scene("plastic").build())
     cam = scenes.furnace_camera(32, 32)
     p = scenes.pt_params(spp=16, sampler="regular", termination="russian-roulette", path_length=3, seed=14)
     plain, sp = _render(gs, cam, p)
