@@ -44,9 +44,11 @@ def args_():
     p.add_argument("--no-extras", action="store_true", help="skip the primary-ray and path-tracing side metrics")
     p.add_argument("--c4-only", action="store_true",
                    help="only the guided-vs-plain measurement on the 64-scene batch set (one JSON line)")
-    p.add_argument("--c4-spp", type=int, default=256)
-    p.add_argument("--c4-ref-spp", type=int, default=4096)
+    p.add_argument("--c4-spp", type=int, default=1024)
+    p.add_argument("--c4-ref-spp", type=int, default=2048)
     p.add_argument("--c4-steps", type=int, default=32)
+    p.add_argument("--c4-mix", type=float, default=0.5)
+    p.add_argument("--c4-depth", type=int, default=0, help="guided_depth of the C4 guides (0: every vertex)")
     p.add_argument("--guide-train-only", action="store_true",
                    help="only the guide's training-step times on 2^18 device records (one JSON line)")
     return p.parse_args()
@@ -180,54 +182,7 @@ def guided_vs_plain(spt, scenes, dev, torch, name, sb, spp, ref_spp, steps, seed
             name + "_equal_time_relmse_ratio_plain_over_guided": round((ep * tp) / (eg * tg), 4)}
 
 
-def guided_batch_sample(spt, scenes, dev, torch, n=8, res_cap=256, spp=1024, ref_spp=16384, steps=32):
-    """Guided vs plain on the first `n` scenes of the 64-scene batch set (resolution capped at
-    `res_cap`^2, `spp` samples, max length 5): the same equal-time relMSE ratio as guided_vs_plain,
-    with (relMSE x wall time) summed over the scenes, each against a `ref_spp` plain render.  Each
-    scene trains a fresh guide (`steps` Adam steps of 2^16 records, mix 0.5) over the unit box."""
-    import numpy as np
-
-    def relmse(a, b):
-        return float(np.mean((a - b) ** 2 / (b ** 2 + 1e-2)))
-
-    ep = eg = 0.0
-    segs_p = segs_g = 0
-    per_scene = []
-    for i, (sb, cam0, _, _) in enumerate(scenes.batched_scenes()[:n]):
-        res = min(cam0.width, res_cap)
-        cam = scenes.box_camera(res, res)
-        gs = spt.GpuScene(dev, sb.build())
-        img = torch.empty(res * res * 3, dtype=torch.float32, device="cuda")
-
-        def render(k, seed, guide=None):
-            p = scenes.pt_params(spp=k, sampler="jittered", termination="max-length", path_length=5, seed=seed)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            if guide is None:
-                st = gs.pathtrace_device(cam, p, img.data_ptr())
-            else:
-                st = gs.pathtrace_guided_device(cam, p, guide, img.data_ptr())
-            torch.cuda.synchronize()
-            return img.cpu().numpy().copy(), time.perf_counter() - t0, st.segments
-
-        render(16, 1)
-        ref, _, _ = render(ref_spp, 99)
-        plain, tp, sp = render(spp, 7 + i)
-        g = spt.Guide(dev, spt.guide_config(batch=1 << 16, max_steps=steps, mix=0.5, seed=7 + i))
-        guided, tg, sg = render(spp, 7 + i, g)
-        g.close()
-        gs.close()
-        a, b = relmse(plain, ref) * tp, relmse(guided, ref) * tg
-        ep, eg = ep + a, eg + b
-        segs_p, segs_g = segs_p + sp, segs_g + sg
-        per_scene.append(round(a / b, 3))
-    key = "guided_batch_first%d_%dpx_%dspp" % (n, res_cap, spp)
-    return {key + "_equal_time_relmse_ratio_plain_over_guided": round(ep / eg, 4),
-            key + "_per_scene_ratios": per_scene,
-            key + "_segments_guided_over_plain": round(segs_g / segs_p, 4)}
-
-
-def guided_c4(spt, scenes, dev, torch, spp=256, ref_spp=4096, batch=1 << 18, steps=32, mix=0.5, n=64):
+def guided_c4(spt, scenes, dev, torch, spp=1024, ref_spp=2048, batch=1 << 18, steps=32, mix=0.5, depth=0, n=64):
     """Guided vs plain path tracing on the whole 64-scene batch set (each scene at its own resolution,
     128^2 to 1024^2, max path length 5), the guide configured as specified: batch 2^18 training records,
     Adam lr 1e-2, mix 0.5.  Per scene: a plain render and a guided render of `spp` samples (the guided
@@ -239,13 +194,16 @@ def guided_c4(spt, scenes, dev, torch, spp=256, ref_spp=4096, batch=1 << 18, ste
     their mean R is (R1 - R2)^2 / 4 per pixel, and subtracting it from each arm's relMSE gives the
     debiased figures (`..._debiased`).  The equal-time ratio is sum(relMSE_plain * t_plain) /
     sum(relMSE_guided * t_guided) over the scenes (relMSE falls as 1 / time), > 1 when guiding wins;
-    the geometric mean of the per-scene ratios is reported beside it."""
+    the geometric mean of the per-scene ratios is reported beside it.  `depth` > 0 guides only the
+    first `depth` vertices of a path (guided_depth); `..._nonfinite_pixels` counts NaN or infinite
+    values over all guided images (0 expected)."""
     import math
 
     def relmse(a, b):
         return float(torch.mean((a - b) ** 2 / (b * b + 1e-2)).item())
 
     rows = []
+    nonfinite = 0
     for i, (sb, cam, _, desc) in enumerate(scenes.batched_scenes()[:n]):
         gs = spt.GpuScene(dev, sb.build())
         npx = cam.width * cam.height
@@ -268,10 +226,11 @@ def guided_c4(spt, scenes, dev, torch, spp=256, ref_spp=4096, batch=1 << 18, ste
         ref = 0.5 * (r1 + r2)
         ref_noise = float(torch.mean(0.25 * (r1 - r2) ** 2 / (ref * ref + 1e-2)).item())
         plain, tp = render(spp, 7 + i)
-        g = spt.Guide(dev, spt.guide_config(batch=batch, max_steps=steps, mix=mix, seed=7 + i))
+        g = spt.Guide(dev, spt.guide_config(batch=batch, max_steps=steps, mix=mix, seed=7 + i, guided_depth=depth))
         guided, tg = render(spp, 7 + i, g)
         g.close()
         gs.close()
+        nonfinite += int((~torch.isfinite(guided)).sum().item())
         ep, eg = relmse(plain, ref), relmse(guided, ref)
         rows.append((desc, ep, eg, tp, tg, ref_noise))
         del r1, r2, ref, plain, guided
@@ -287,7 +246,8 @@ def guided_c4(spt, scenes, dev, torch, spp=256, ref_spp=4096, batch=1 << 18, ste
            key + "_per_scene_ratios": [round(x, 3) for x in per],
            key + "_wall_s_plain": round(sum(r[3] for r in rows), 3),
            key + "_wall_s_guided": round(sum(r[4] for r in rows), 3),
-           key + "_reference_spp": ref_spp, key + "_guide": {"batch": batch, "steps": steps, "mix": mix}}
+           key + "_reference_spp": ref_spp, key + "_nonfinite_pixels": nonfinite,
+           key + "_guide": {"batch": batch, "steps": steps, "mix": mix, "guided_depth": depth}}
     by_kind = {}
     for r, x in zip(rows, per):
         by_kind.setdefault(r[0].split(", ")[-1].split(" ")[0], []).append(x)
@@ -409,8 +369,8 @@ def main():
         return
     if a.c4_only:
         dev = spt.Device(local)
-        print(json.dumps(guided_c4(spt, scenes, dev, torch, spp=a.c4_spp, ref_spp=a.c4_ref_spp, steps=a.c4_steps)),
-              flush=True)
+        print(json.dumps(guided_c4(spt, scenes, dev, torch, spp=a.c4_spp, ref_spp=a.c4_ref_spp, steps=a.c4_steps,
+                                   mix=a.c4_mix, depth=a.c4_depth)), flush=True)
         dev.close()
         return
     if world > 1:
@@ -610,8 +570,8 @@ def main():
                                       scenes.window_room_scene(0.1), 16384, 262144, 32, seeds=tuple(range(7, 15))))
         extras.update(guided_vs_plain(spt, scenes, dev, torch, "guided_small_light_128x128",
                                       scenes.small_light_box_scene(), 4096, 16384, 32, seeds=(7,)))
-        # guided rendering on a sample of the batch set (box with a 0.25 x 0.25 ceiling light)
-        extras.update(guided_batch_sample(spt, scenes, dev, torch))
+        # guided rendering on the whole 64-scene batch set, equal-time relMSE against plain
+        extras.update(guided_c4(spt, scenes, dev, torch))
         # the guide's optimiser step at the configured batch of 2^18 records
         extras.update(guide_train_steps(spt, abi, dev, torch))
         out["submetrics"] = extras

@@ -264,7 +264,8 @@ __device__ __forceinline__ V3 mixture_sample(const Lobe (&lb)[kLobes], float u0,
     float acc = lb[0].w;
     while (k < kLobes - 1 && u0 >= acc) acc += lb[++k].w;
     const Lobe& l = lb[k];
-    const float w = 1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * l.kappa)) / l.kappa;
+    // u1 = 0 with e^{-2 kappa} underflowing gives log(0): the cosine's limit there is -1
+    const float w = fmaxf(1.0f + logf(u1 + (1.0f - u1) * expf(-2.0f * l.kappa)) / l.kappa, -1.0f);
     const float s = sqrtf(fmaxf(0.0f, 1.0f - w * w));
     const float phi = 2.0f * kPi * u2;
     // frame around mu
@@ -325,7 +326,10 @@ __device__ __forceinline__ V3 cached_mixture_sample(const float* entry, float u0
     }
     const float mx = __ldg(entry + kLobes * kMuX + k), my = __ldg(entry + kLobes * kMuY + k);
     const float mz = __ldg(entry + kLobes * kMuZ + k), kappa = __ldg(entry + kLobes * kKappa + k);
-    const float w = __fmaf_rn(__logf(__fmaf_rn(1.0f - u1, __expf(-2.0f * kappa), u1)), __frcp_rn(kappa), 1.0f);
+    // The uniforms include 0: with u1 = 0 and e^{-2 kappa} underflowing (kappa above about 44) the
+    // logarithm is -inf, and the cosine takes its limit -1 instead of turning the direction into NaN.
+    const float w =
+        fmaxf(__fmaf_rn(__logf(__fmaf_rn(1.0f - u1, __expf(-2.0f * kappa), u1)), __frcp_rn(kappa), 1.0f), -1.0f);
     const float s = sqrtf(fmaxf(0.0f, __fmaf_rn(-w, w, 1.0f)));
     float sn, cs;
     __sincosf(2.0f * kPi * u2, &sn, &cs);

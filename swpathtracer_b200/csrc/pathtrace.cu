@@ -405,7 +405,8 @@ __global__ void __launch_bounds__(256, 3) k_shade(Wave W, Counters* __restrict__
                     const V3 beta0 = beta;
                     beta = ((beta * f) * wi.y) / pdf;              // pathtracer.cpp:52-54
                     if ((beta.x == 0.0f && beta.y == 0.0f && beta.z == 0.0f) ||
-                        (!J.rr && depth + 1 >= J.path_length)) {   // the next trace would return 0
+                        (!J.rr && depth + 1 >= J.path_length) ||  // the next trace would return 0
+                        (GUIDED && !(isfinite(beta.x) && isfinite(beta.y) && isfinite(beta.z)))) {
                         done = true;
                     } else {
                         if (GUIDED && RECORDS && gi != kNoRec && c.train_on) {
@@ -472,14 +473,28 @@ __global__ void k_continue(Wave W, const Counters* __restrict__ ctr, uint32_t ma
 }
 
 // Training weight of every record: luminance of (radiance gathered after the record / throughput at it),
-// i.e. the path's estimate of f cos Li / p at the record.
+// i.e. the path's estimate of f cos Li / p at the record, clamped to [0, 1e3] (NaN -> 0).  A record
+// with a non-finite position, normal or direction (none is expected; one would turn every parameter
+// of the guide into NaN through its gradient) becomes a zero-weight record at the origin.
 __global__ void k_record_weights(float4* __restrict__ rec, const float4* __restrict__ recx, uint32_t n) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 b = recx[2 * i], sx = recx[2 * i + 1];
         const float r = b.x > 0.0f ? sx.x / b.x : 0.0f, g = b.y > 0.0f ? sx.y / b.y : 0.0f,
                     bl = b.z > 0.0f ? sx.z / b.z : 0.0f;
         const float w = 0.2126f * r + 0.7152f * g + 0.0722f * bl;
-        rec[4 * i].w = fminf(fmaxf(w, 0.0f), 1e3f);
+        bool finite = true;
+        for (int k = 0; k < 4; ++k) {
+            const float4 f = rec[4 * i + k];
+            finite = finite && isfinite(f.x) && isfinite(f.y) && isfinite(f.z);
+        }
+        if (finite) {
+            rec[4 * i].w = fminf(fmaxf(w, 0.0f), 1e3f);
+        } else {
+            rec[4 * i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            rec[4 * i + 1] = make_float4(0.0f, 1.0f, 0.0f, 0.0f);
+            rec[4 * i + 2] = make_float4(0.0f, 1.0f, 0.0f, 0.0f);
+            rec[4 * i + 3] = make_float4(0.0f, 1.0f, 0.0f, 0.0f);
+        }
     }
 }
 

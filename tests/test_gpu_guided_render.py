@@ -83,6 +83,25 @@ def test_guided_batch_scene_gains(device):
     assert e_guided < 0.8 * e_plain, (desc, e_guided, e_plain)
 
 
+@pytest.mark.parametrize("idx,seed,depth", [(52, 59, 1), (45, 52, 0)])
+def test_guided_batch_scene_stays_finite(device, idx, seed, depth):
+    """Two scenes of the 64-scene batch set at their full sizes and 1024 spp: a rough conductor (401 x
+    401, 238k triangles) whose training once turned every guide parameter into NaN with this seed, and
+    a narrow coated stack (718 x 718) whose guided samples once left NaN pixels.  Both came from the
+    vMF sampler's log(0) at a uniform of exactly 0 (one in 2^24) under a narrow lobe."""
+    sb, cam, _, desc = scenes.batched_scenes()[idx]
+    gs = spt.GpuScene(device, sb.build())
+    p = scenes.pt_params(spp=1024, sampler="jittered", termination="max-length", path_length=5, seed=7 + idx)
+    plain, _ = _render(gs, cam, p)
+    g = spt.Guide(device, spt.guide_config(batch=1 << 18, max_steps=32, mix=0.5, seed=seed, guided_depth=depth))
+    guided, _ = _render(gs, cam, p, g)
+    grid, mlp = g.get_params()
+    g.close()
+    assert np.isfinite(grid).all() and np.isfinite(mlp).all(), desc
+    assert np.isfinite(guided).all(), (desc, int((~np.isfinite(guided)).sum()))
+    assert abs(float(guided.mean()) - float(plain.mean())) <= 0.02 * float(plain.mean()), desc
+
+
 @pytest.mark.parametrize("mix", [0.5, 0.9])
 def test_guided_window_room_is_unbiased_and_less_noisy(device, mix):
     # light enters through a 0.1 x 0.1 window: the sampled lobe and its density (the lobe cache) must
