@@ -46,7 +46,7 @@ def args_():
                    help="only the guided-vs-plain measurement on the 64-scene batch set (one JSON line)")
     p.add_argument("--c4-spp", type=int, default=1024)
     p.add_argument("--c4-ref-spp", type=int, default=2048)
-    p.add_argument("--c4-steps", type=int, default=32)
+    p.add_argument("--c4-steps", type=int, default=256)
     p.add_argument("--c4-mix", type=float, default=0.5)
     p.add_argument("--c4-depth", type=int, default=0, help="guided_depth of the C4 guides (0: every vertex)")
     p.add_argument("--guide-train-only", action="store_true",
@@ -182,7 +182,7 @@ def guided_vs_plain(spt, scenes, dev, torch, name, sb, spp, ref_spp, steps, seed
             name + "_equal_time_relmse_ratio_plain_over_guided": round((ep * tp) / (eg * tg), 4)}
 
 
-def guided_c4(spt, scenes, dev, torch, spp=1024, ref_spp=2048, batch=1 << 18, steps=32, mix=0.5, depth=0, n=64):
+def guided_c4(spt, scenes, dev, torch, spp=1024, ref_spp=2048, batch=1 << 18, steps=256, mix=0.5, depth=0, n=64):
     """Guided vs plain path tracing on the whole 64-scene batch set (each scene at its own resolution,
     128^2 to 1024^2, max path length 5), the guide configured as specified: batch 2^18 training records,
     Adam lr 1e-2, mix 0.5.  Per scene: a plain render and a guided render of `spp` samples (the guided

@@ -311,7 +311,8 @@ typedef struct spt_guide_config {
                                       least one, at most max_steps (0: the guide stays frozen) */
     float mix;                     /* probability of sampling the guiding distribution */
     uint64_t seed;                 /* parameter initialisation */
-    uint32_t cache_res;            /* cells per axis of the lobe cache guided renders sample: 4..64, 0 = 32 */
+    uint32_t cache_res;            /* cells per axis of the lobe cache guided renders sample: 4..128, 0 = 128
+                                      (6 normal axes per cell, 192 bytes per entry: 2.4 GB at 128) */
     uint32_t train_path;           /* SPT_GUIDE_TRAIN_TCGEN05 (0): the MLP's training GEMMs on the 5th-gen
                                       tensor cores, tiles of 128 records with fp32 accumulators in tensor
                                       memory; SPT_GUIDE_TRAIN_MMA_SYNC (1): warp-level mma.sync tiles of

@@ -278,7 +278,7 @@ def autotune(device, jobs, cache_path=None):
     return t
 
 
-def guide_config(box_min=(0, 0, 0), box_max=(1, 1, 1), lr=1e-2, batch=1 << 18, max_steps=64, mix=0.5, seed=1,
+def guide_config(box_min=(0, 0, 0), box_max=(1, 1, 1), lr=1e-2, batch=1 << 18, max_steps=256, mix=0.5, seed=1,
                  cache_res=0, train_path=abi.GUIDE_TRAIN_TCGEN05, guided_depth=0):
     """train_path: abi.GUIDE_TRAIN_TCGEN05 (the training GEMMs on tcgen05 with tensor-memory
     accumulators, tiles of 128 records) or abi.GUIDE_TRAIN_MMA_SYNC (warp-level mma.sync).

@@ -68,9 +68,12 @@ __global__ void __launch_bounds__(256) k_encode(const __grid_constant__ Model M,
 // The network inputs of the guide cache: entry ((iz * R + iy) * R + ix) * 6 + bin is the centre of
 // cell (ix, iy, iz) of an R^3 grid over the box, with the normal +x, -x, +y, -y, +z, -z for bin 0..5
 // (wo = the normal).
-__global__ void k_cache_inputs(Model M, uint32_t R, float4* __restrict__ in) {
-    const uint32_t n = R * R * R * 6;
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+// Network inputs of cache entries first .. first + n - 1 of the list (of the whole cache when list is
+// NULL): the cell centre and the axis normal, which also stands in for the view direction.
+__global__ void k_cache_inputs(Model M, uint32_t R, const uint32_t* __restrict__ list, uint32_t first, uint32_t n,
+                               float4* __restrict__ in) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint32_t e = list ? list[first + j] : first + j;
         const uint32_t bin = e % 6, cell = e / 6;
         const uint32_t ix = cell % R, iy = (cell / R) % R, iz = cell / (R * R);
         const float x = M.lo[0] + (ix + 0.5f) / (R * M.inv_ext[0]);
@@ -78,19 +81,21 @@ __global__ void k_cache_inputs(Model M, uint32_t R, float4* __restrict__ in) {
         const float z = M.lo[2] + (iz + 0.5f) / (R * M.inv_ext[2]);
         const float sgn = (bin & 1u) ? -1.0f : 1.0f;
         const float4 nrm = make_float4(bin < 2 ? sgn : 0.0f, (bin >> 1) == 1 ? sgn : 0.0f, bin >= 4 ? sgn : 0.0f, 0.0f);
-        in[3 * e] = make_float4(x, y, z, 0.0f);
-        in[3 * e + 1] = nrm;
-        in[3 * e + 2] = nrm;
+        in[3 * j] = make_float4(x, y, z, 0.0f);
+        in[3 * j + 1] = nrm;
+        in[3 * j + 2] = nrm;
     }
 }
 
-// Decoded lobes {mu.xyz, kappa, w} -> field-major cache entries of mu.xyz, kappa, w, w * C(kappa)
-// (guiding.cuh).
-__global__ void k_cache_pack(const float* __restrict__ raw, uint32_t n, float* __restrict__ out) {
+// Decoded lobes {mu.xyz, kappa, w} of n listed entries -> their field-major cache entries of mu.xyz,
+// kappa, w, w * C(kappa) (guiding.cuh).
+__global__ void k_cache_pack(const float* __restrict__ raw, uint32_t n, const uint32_t* __restrict__ list,
+                             uint32_t first, float* __restrict__ out) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n * kLobes; i += gridDim.x * blockDim.x) {
         const float* l = raw + 5ull * i;
-        const uint32_t lobe = i % kLobes;
-        float* o = out + static_cast<uint64_t>(kCacheEntry) * (i / kLobes) + lobe;
+        const uint32_t lobe = i % kLobes, j = i / kLobes;
+        const uint32_t e = list ? list[first + j] : first + j;
+        float* o = out + static_cast<uint64_t>(kCacheEntry) * e + lobe;
         const float kappa = l[3];
         o[kLobes * kMuX] = l[0];
         o[kLobes * kMuY] = l[1];
@@ -98,6 +103,22 @@ __global__ void k_cache_pack(const float* __restrict__ raw, uint32_t n, float* _
         o[kLobes * kKappa] = kappa;
         o[kLobes * kWeight] = l[4];
         o[kLobes * kWeightC] = l[4] * (kappa / (2.0f * kPi * (1.0f - expf(-2.0f * kappa))));
+    }
+}
+
+// The touched entries, in any order (each entry's refresh is independent of the others), and their
+// count at list[n]; warp-aggregated so one atomic serves a warp's hits.
+__global__ void k_cache_select(const uint8_t* __restrict__ touched, uint32_t n, uint32_t* __restrict__ list) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint32_t e = base + threadIdx.x;
+        const bool hit = e < n && touched[e] != 0;
+        const unsigned mask = __ballot_sync(0xFFFFFFFFu, hit);
+        uint32_t first = 0;
+        if (lane == 0 && mask) first = atomicAdd(list + n, static_cast<uint32_t>(__popc(mask)));
+        first = __shfl_sync(0xFFFFFFFFu, first, 0);
+        if (hit) list[first + __popc(mask & ((1u << lane) - 1u))] = e;
     }
 }
 
@@ -526,16 +547,22 @@ spt_status Guide::alloc(spt_context* c, const spt_guide_config& cfg_) {
     // nothing: the training buffers of one batch, the lobe cache and its inference scratch
     if ((st = ensure_train_buffers(cfg.batch)) != SPT_OK) return st;
     cache_res = cfg.cache_res ? cfg.cache_res : kCacheRes;
-    const uint32_t n_cache = cache_res * cache_res * cache_res * 6;
-    if ((st = ensure_features(n_cache)) != SPT_OK) return st;
+    n_cache = cache_res * cache_res * cache_res * 6;
+    const uint32_t chunk = std::min(n_cache, kCacheChunk);
+    if ((st = ensure_features(chunk)) != SPT_OK) return st;
     SPT_CUDA(ctx, cudaMalloc(&cache, static_cast<size_t>(n_cache) * kCacheEntry * sizeof(float)));
-    SPT_CUDA(ctx, cudaMalloc(&cache_raw, static_cast<size_t>(n_cache) * kOutUsed * sizeof(float)));
-    SPT_CUDA(ctx, cudaMalloc(&cache_in, static_cast<size_t>(n_cache) * 3 * sizeof(float4)));
-    return refresh();
+    SPT_CUDA(ctx, cudaMalloc(&cache_raw, static_cast<size_t>(chunk) * kOutUsed * sizeof(float)));
+    SPT_CUDA(ctx, cudaMalloc(&cache_in, static_cast<size_t>(chunk) * 3 * sizeof(float4)));
+    SPT_CUDA(ctx, cudaMalloc(&touched, n_cache));
+    SPT_CUDA(ctx, cudaMemsetAsync(touched, 0, n_cache, ctx->stream));
+    SPT_CUDA(ctx, cudaMalloc(&cache_list, (static_cast<size_t>(n_cache) + 1) * sizeof(uint32_t)));
+    if ((st = refresh()) != SPT_OK) return st;
+    return refresh_cache();
 }
 
-// bf16 copies of the current master parameters
+// bf16 copies of the current master parameters (which have changed: a new parameter version)
 spt_status Guide::refresh() {
+    ++version;
     k_stage<<<(kMlpParams + 255) / 256, 256, 0, ctx->stream>>>(mlp_master, smem_image);
     k_to_bf16<<<4096, 256, 0, ctx->stream>>>(grid_master, grid_bf16, kGridParams);
     SPT_CUDA(ctx, cudaGetLastError());
@@ -553,13 +580,31 @@ spt_status Guide::ensure_features(uint32_t n) {
 }
 
 spt_status Guide::refresh_cache() {
-    const uint32_t n = cache_res * cache_res * cache_res * 6;
-    k_cache_inputs<<<256, 256, 0, ctx->stream>>>(model, cache_res, cache_in);
-    SPT_CUDA(ctx, cudaGetLastError());
-    spt_status st = infer(cache_in, n, cache_raw, ctx->stream);
-    if (st != SPT_OK) return st;
-    k_cache_pack<<<256, 256, 0, ctx->stream>>>(cache_raw, n, cache);
-    SPT_CUDA(ctx, cudaGetLastError());
+    if (cache_version == version) return SPT_OK;
+    uint32_t n = n_cache;
+    const uint32_t* list = nullptr;
+    if (touched_any) {
+        // only the entries guided renders have read; the count comes back to the host to size the passes
+        SPT_CUDA(ctx, cudaMemsetAsync(cache_list + n_cache, 0, sizeof(uint32_t), ctx->stream));
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+        const unsigned g = static_cast<unsigned>(std::min<uint64_t>((n_cache + 255) / 256, 8ull * sms));
+        k_cache_select<<<g, 256, 0, ctx->stream>>>(touched, n_cache, cache_list);
+        SPT_CUDA(ctx, cudaGetLastError());
+        SPT_CUDA(ctx, cudaMemcpyAsync(&n, cache_list + n_cache, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        SPT_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        list = cache_list;
+    }
+    for (uint32_t first = 0; first < n; first += kCacheChunk) {
+        const uint32_t c = std::min(kCacheChunk, n - first);
+        k_cache_inputs<<<256, 256, 0, ctx->stream>>>(model, cache_res, list, first, c, cache_in);
+        SPT_CUDA(ctx, cudaGetLastError());
+        spt_status st = infer(cache_in, c, cache_raw, ctx->stream);
+        if (st != SPT_OK) return st;
+        k_cache_pack<<<256, 256, 0, ctx->stream>>>(cache_raw, c, list, first, cache);
+        SPT_CUDA(ctx, cudaGetLastError());
+    }
+    cache_version = version;
     return SPT_OK;
 }
 
@@ -648,6 +693,7 @@ spt_status Guide::step(const float4* d_rec, uint32_t n, float* loss) {
     spt_status st = gradients(d_rec, n);
     if (st != SPT_OK) return st;
     ++steps;
+    ++version;
     const float c1 = 1.0f - std::pow(0.9f, static_cast<float>(steps));
     const float c2 = 1.0f - std::pow(0.99f, static_cast<float>(steps));
     k_adam_sparse<<<4096, 256, 0, ctx->stream>>>(grid_master, grid_m, grid_v, grid_grad, grid_bf16, kGridParams, cfg.lr,

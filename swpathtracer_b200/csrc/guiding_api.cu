@@ -31,11 +31,11 @@ spt_status spt_guide_create(spt_context* ctx, const spt_guide_config* cfg, spt_g
     *out = nullptr;
     if (!(cfg->lr > 0.0f) || cfg->batch == 0 || !(cfg->mix >= 0.0f && cfg->mix <= 1.0f))
         return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "guide config: lr > 0, batch > 0, mix in [0, 1]");
-    if ((cfg->cache_res != 0 && (cfg->cache_res < 4 || cfg->cache_res > 64)) ||
+    if ((cfg->cache_res != 0 && (cfg->cache_res < 4 || cfg->cache_res > 128)) ||
         (cfg->train_path != SPT_GUIDE_TRAIN_TCGEN05 && cfg->train_path != SPT_GUIDE_TRAIN_MMA_SYNC) ||
         cfg->reserved != 0)
         return fail(ctx, SPT_ERR_INVALID_ARGUMENT,
-                    "guide config: cache_res 0 or 4..64, train_path 0 or 1, reserved 0");
+                    "guide config: cache_res 0 or 4..128, train_path 0 or 1, reserved 0");
     SPT_CUDA(ctx, cudaSetDevice(ctx->device));
     auto g = std::unique_ptr<spt_guide>(new (std::nothrow) spt_guide());
     if (!g) return SPT_ERR_OUT_OF_MEMORY;

@@ -45,12 +45,22 @@ struct Guide {
     uint32_t* feats = nullptr;
     uint32_t feats_cap = 0;
     // the mixture cached per (cell of a cache_res^3 grid over the box, normal axis): what guided
-    // rendering samples, refreshed after every round of training
-    static constexpr uint32_t kCacheRes = 32;   // cells per axis unless the config names another
+    // rendering samples.  Filled whole when the guide is created; after that a refresh re-evaluates
+    // only the entries guided renders have looked up (touched), kCacheChunk entries per network pass.
+    // An entry not refreshed keeps an earlier mixture of the guide, which sampling and density read
+    // alike, so the estimator stays unbiased; a refresh is skipped while the parameters are unchanged.
+    static constexpr uint32_t kCacheRes = 128;           // cells per axis unless the config names another
+    static constexpr uint32_t kCacheChunk = 1u << 20;    // entries per network pass of a refresh
     uint32_t cache_res = kCacheRes;
-    float* cache = nullptr;        // cache_res^3 * 6 entries of kCacheEntry floats
-    float* cache_raw = nullptr;    // the same entries as decoded lobes (40 floats), before packing
-    float4* cache_in = nullptr;    // the network inputs of the cache entries
+    uint32_t n_cache = 0;          // cache_res^3 * 6
+    float* cache = nullptr;        // n_cache entries of kCacheEntry floats
+    float* cache_raw = nullptr;    // one chunk of entries as decoded lobes (40 floats), before packing
+    float4* cache_in = nullptr;    // the network inputs of one chunk
+    uint8_t* touched = nullptr;    // n_cache flags set by guided shading at every entry it reads
+    uint32_t* cache_list = nullptr;   // the touched entries of a refresh, then their count at [n_cache]
+    bool touched_any = false;      // a guided render has run with this guide (touched is meaningful)
+    uint64_t version = 0;          // bumped by every change of the parameters
+    uint64_t cache_version = ~0ull;   // the parameter version the cache was last refreshed at
 
     spt_status alloc(spt_context* c, const spt_guide_config& cfg);
     spt_status refresh();
@@ -73,6 +83,8 @@ struct Guide {
         if (cache) cudaFree(cache);
         if (cache_raw) cudaFree(cache_raw);
         if (cache_in) cudaFree(cache_in);
+        if (touched) cudaFree(touched);
+        if (cache_list) cudaFree(cache_list);
         for (void* p : train_allocs) cudaFree(p);
         for (void* p : allocations) cudaFree(p);
     }

@@ -71,6 +71,7 @@ struct GuideIO {
     uint32_t rec_cap;
     uint32_t depth;        // vertices at path depth < depth are guided
     const float* cache;    // the guide's mixture per (position cell, normal axis): guide::kCacheEntry floats each
+    uint8_t* touched;      // per cache entry: set when a guided vertex reads it (the next refresh includes it)
     uint32_t cache_res;    // cells per axis over the guide's box
     float lo[3], inv_ext[3];
     float4* rec;           // 4 float4 per record (spt_guide_record layout)
@@ -356,6 +357,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(Wave W, Counters* __restrict__
                                         ? cache_cell(G, pos, nrm)
                                         : kNoRec;
                 const float* entry = G.cache + static_cast<uint64_t>(guide::kCacheEntry) * (gi != kNoRec ? gi : 0u);
+                if (GUIDED && gi != kNoRec) G.touched[gi] = 1;
                 bool sampled = false;
                 if (GUIDED && gi != kNoRec && (!coat || bs.next() < G.mix)) {
                     const GuidedSample gs = coat ? coated_guide_sample(J.S, m, frame, wo, entry, G.mix, bs)
@@ -647,7 +649,9 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
         G.rec_cap = rec_cap;
         G.depth = guide->cfg.guided_depth ? guide->cfg.guided_depth : 0xFFFFFFFFu;
         if ((st = guide->refresh_cache()) != SPT_OK) return st;
+        guide->touched_any = true;
         G.cache = guide->cache;
+        G.touched = guide->touched;
         G.cache_res = guide->cache_res;
         for (int k = 0; k < 3; ++k) {
             G.lo[k] = guide->model.lo[k];
