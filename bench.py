@@ -398,8 +398,24 @@ def main():
     t_box = float(t_tests.double().mean()) - t_tri
     bytes_per_ray = 24.0 * t_box + 36.0 * t_tri + 32.0 + 16.0
 
-    def step():
-        gs.intersect_device(d_rays.data_ptr(), n, d_hits.data_ptr(), 0)
+    # A step is spt_intersect_device's three stages called one by one, so that the traversal kernel's
+    # own time can be bracketed by events inside the timed region: the coherence order of the batch
+    # (four kernels: per-block key histograms, their offsets, the scan of the key totals, the
+    # scatter), the persistent closest-hit kernel in that order, and the gather of the hits back to
+    # the rays' own indices.  All of it runs on the legacy default stream, torch's current stream
+    # here, so the events see the kernels.
+    d_order = torch.empty(2 * n + 1, dtype=torch.int32, device="cuda")
+    d_hits_ordered = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    kernels_per_step = 6
+
+    def step(mid=None):
+        gs.ray_order_device(d_rays.data_ptr(), n, d_order.data_ptr(), 0)
+        if mid:
+            mid[0].record()
+        gs.intersect_ordered_device(d_rays.data_ptr(), d_order.data_ptr(), n, d_hits_ordered.data_ptr(), 0)
+        if mid:
+            mid[1].record()
+        gs.hits_unorder_device(d_order.data_ptr(), n, d_hits_ordered.data_ptr(), d_hits.data_ptr(), 0)
 
     for _ in range(a.warmup):
         step()
@@ -408,13 +424,15 @@ def main():
         dist.barrier()
     clocks = Clocks(local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    mids = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(a.steps)]
     torch.cuda.synchronize()
     ev0.record()
-    for _ in range(a.steps):
-        step()
+    for k in range(a.steps):
+        step(mids[k])
     ev1.record()
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
+    ms_trace = sum(b.elapsed_time(c) for b, c in mids) / a.steps
     clk = clocks.stop()
     if world > 1:
         t = torch.tensor([ms], device="cuda")
@@ -442,7 +460,7 @@ def main():
         e2e = float(t.item()) * world
 
     hbm, peak_kind = peaks()
-    achieved = bytes_per_ray * n / (ms_step / 1000.0) / 1e9
+    achieved = bytes_per_ray * n / (ms_trace / 1000.0) / 1e9
     traffic = None
     prof = {}
     tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
@@ -472,13 +490,15 @@ def main():
                         "kernel_node_visits_per_ray": round(work_nodes / ns, 3),
                         "kernel_box_tests_per_ray": round(8.0 * work_nodes / ns, 3),
                         "kernel_prim_tests_per_ray": round(work_prims / ns, 3),
-                        "dram_frac": (round(traffic / (ms_step / 1000.0) / 1e9 / hbm, 4) if traffic else None),
+                        "kernel_ms": round(ms_trace, 4), "kernel": "k_intersect_df_ordered",
+                        "ordering_and_gather_ms": round(ms_step - ms_trace, 4),
+                        "dram_frac": (round(traffic / (ms_trace / 1000.0) / 1e9 / hbm, 4) if traffic else None),
                         "issue_active_frac": prof.get("issue_active"),
                         "lanes_per_instruction": prof.get("lanes_per_instruction"),
                         "profile": prof.get("source")},
            "e2e": {"value": round(e2e, 3), "unit": "Mrays/s", "h2d_bytes_per_step": n * 24,
                    "d2h_bytes_per_step": n * 16},
-           "gpu_launches": a.steps,
+           "gpu_launches": kernels_per_step * a.steps,
            "bvh_build_ms": round(build_ms, 1),
            "clocks": clk}
 

@@ -222,8 +222,29 @@ spt_status spt_intersect(spt_context* ctx, const spt_scene* scene, const float* 
  * moves a quarter fewer bytes to the device than the padded 32-byte layout. */
 spt_status spt_intersect_packed(spt_context* ctx, const spt_scene* scene, const float* rays, uint64_t n,
                                 spt_hit* hits, uint32_t* tests, uint32_t* nhits);
+/* Device rays (8 floats each) and hits, on `stream` (NULL: the legacy default stream).  A batch of at
+ * least 2^21 rays on a scene with the 8-wide tree is traced in coherence order (neighbouring rays
+ * enter the scene's box near each other with similar directions; misses last), which makes the
+ * traversal's warps diverge less; the hits are the same in any order.  Its working buffers belong to
+ * the stream (one set per stream for up to eight streams; a ninth stream's batches keep their own
+ * order).  The three stages are also callable one by one (n < 2^32 rays): */
 spt_status spt_intersect_device(spt_context* ctx, const spt_scene* scene, const float* d_rays,
                                 uint64_t n, spt_hit* d_hits, void* stream);
+/* 1. The coherence order of n device rays (8 floats each) into d_order (2n + 1 entries): d_order[2n]
+ *    = m, the number of rays that meet the scene's root box; d_order[k], k < m, the index of the k-th
+ *    of them to trace; d_order[n + i] the place of ray i in that order, or 0xFFFFFFFF for a ray the
+ *    root box test rejects (SPT_ERR_UNSUPPORTED when eight other streams hold the working buffers). */
+spt_status spt_ray_order_device(spt_context* ctx, const spt_scene* scene, const float* d_rays, uint64_t n,
+                                uint32_t* d_order, void* stream);
+/* 2. Closest hits of the rays d_rays[d_order[k]] into d_hits_ordered[k], k < d_order[2n], on the
+ *    persistent 8-wide traversal (SPT_ERR_UNSUPPORTED for a scene on another traversal). */
+spt_status spt_intersect_ordered_device(spt_context* ctx, const spt_scene* scene, const float* d_rays,
+                                        const uint32_t* d_order, uint64_t n, spt_hit* d_hits_ordered,
+                                        void* stream);
+/* 3. d_hits[i] = d_hits_ordered[d_order[n + i]], or the miss record (t = +inf, SPT_MISS, u = v = 0)
+ *    for a ray without a place: every hit back at its ray's index. */
+spt_status spt_hits_unorder_device(spt_context* ctx, const uint32_t* d_order, uint64_t n,
+                                   const spt_hit* d_hits_ordered, spt_hit* d_hits, void* stream);
 /* The reference's own traversal order (unordered, unpruned, depth first): per-ray test counts
  * (box + primitive tests, and the primitive tests alone) and, when d_ref_hits is not NULL, the
  * hit that traversal keeps.  Any output may be NULL. */

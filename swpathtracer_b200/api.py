@@ -191,8 +191,27 @@ class GpuScene:
         return dict(hits=hits, tests=tests, nhits=nh)
 
     def intersect_device(self, d_rays, n, d_hits, stream=0):
+        """Closest hits of n device rays (8 floats each); a batch of at least 2^21 rays is traced in
+        coherence order (the same hits)."""
         self.dev.check(self.lib.spt_intersect_device(self.dev.h, self.h, d_rays, n, d_hits, stream),
                        "spt_intersect_device")
+
+    def ray_order_device(self, d_rays, n, d_order, stream=0):
+        """Stage 1 of intersect_device: the coherence order of n device rays into d_order (2n + 1
+        uint32: the rays that meet the scene's box in order, then each ray's place in it or
+        0xFFFFFFFF, then the number of those rays)."""
+        self.dev.check(self.lib.spt_ray_order_device(self.dev.h, self.h, d_rays, n, d_order, stream),
+                       "spt_ray_order_device")
+
+    def intersect_ordered_device(self, d_rays, d_order, n, d_hits_ordered, stream=0):
+        """Stage 2: closest hits of the rays d_rays[d_order[k]] into d_hits_ordered[k]."""
+        self.dev.check(self.lib.spt_intersect_ordered_device(self.dev.h, self.h, d_rays, d_order, n, d_hits_ordered,
+                                                             stream), "spt_intersect_ordered_device")
+
+    def hits_unorder_device(self, d_order, n, d_hits_ordered, d_hits, stream=0):
+        """Stage 3: d_hits[i] = d_hits_ordered[d_order[n + i]]."""
+        self.dev.check(self.lib.spt_hits_unorder_device(self.dev.h, d_order, n, d_hits_ordered, d_hits, stream),
+                       "spt_hits_unorder_device")
 
     def traversal_work_device(self, d_rays, n, d_hits):
         """The closest-hit kernel's own work on n device rays: (8-wide node visits, primitive tests)."""

@@ -37,6 +37,27 @@ spt_status scratch(spt_context* ctx, int i, size_t bytes, void** out) {
     return SPT_OK;
 }
 
+spt_status stream_scratch(spt_context* ctx, cudaStream_t s, size_t bytes, void** out) {
+    *out = nullptr;
+    int k = -1;
+    for (int i = 0; i < spt_context::kStreamScratch && k < 0; ++i)
+        if (ctx->sscratch[i] && ctx->sscratch_stream[i] == s) k = i;
+    for (int i = 0; i < spt_context::kStreamScratch && k < 0; ++i)
+        if (!ctx->sscratch[i]) k = i;
+    if (k < 0) return SPT_OK;
+    if (ctx->sscratch_bytes[k] < bytes) {
+        // cudaFree waits for the device, so no work still reads the old buffer
+        if (ctx->sscratch[k]) SPT_CUDA(ctx, cudaFree(ctx->sscratch[k]));
+        ctx->sscratch[k] = nullptr;
+        ctx->sscratch_bytes[k] = 0;
+        SPT_CUDA(ctx, cudaMalloc(&ctx->sscratch[k], bytes));
+        ctx->sscratch_bytes[k] = bytes;
+    }
+    ctx->sscratch_stream[k] = s;
+    *out = ctx->sscratch[k];
+    return SPT_OK;
+}
+
 spt_status pinned(spt_context* ctx, size_t bytes, void** out) {
     if (ctx->pinned_bytes < bytes) {
         if (ctx->pinned) SPT_CUDA(ctx, cudaFreeHost(ctx->pinned));
@@ -255,6 +276,8 @@ spt_status spt_destroy(spt_context* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (int i = 0; i < spt_context::kScratchSlots; ++i)
         if (ctx->scratch[i]) cudaFree(ctx->scratch[i]);
+    for (int i = 0; i < spt_context::kStreamScratch; ++i)
+        if (ctx->sscratch[i]) cudaFree(ctx->sscratch[i]);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->d_fetch) cudaFree(ctx->d_fetch);

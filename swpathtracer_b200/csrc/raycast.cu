@@ -51,6 +51,24 @@ __global__ void __launch_bounds__(kBlock, 10) k_intersect_df(DevScene S, const f
         });
 }
 
+// The same kernel over a batch in coherence order (ray_order.cu): the k-th ray it takes is order[k],
+// for k below order[2n] (the rays that meet the root box), and its hit goes to place k of
+// hits_ordered, so that neighbouring lanes write neighbouring hits (scattered 16-byte stores cost
+// partial-sector writes in DRAM).
+template <int STRIDE>
+__global__ void __launch_bounds__(kBlock, 10) k_intersect_df_ordered(DevScene S, const float* __restrict__ rays,
+                                                                 const uint32_t* __restrict__ order, uint64_t n,
+                                                                 spt_hit* __restrict__ hits_ordered, uint32_t* status,
+                                                                 unsigned long long* next) {
+    const uint64_t traced = __ldg(order + 2 * n);
+    persistent_trace(
+        S, traced, next, status, [&](uint64_t k, V3& o, V3& d) { load_ray<STRIDE, true>(rays, __ldg(order + k), o, d); },
+        [&](uint64_t k, const Hit1& h) {
+            __stcs(reinterpret_cast<float4*>(hits_ordered + k),
+                   make_float4(h.t, __uint_as_float(h.found ? slot_prim(S, h.slot) : SPT_MISS), h.u, h.v));
+        });
+}
+
 // The same kernel with its own work counted (node visits, primitive tests): the work behind the
 // throughput of k_intersect_df, for comparison with the reference traversal's test counts.
 __global__ void __launch_bounds__(kBlock, 10) k_intersect_df_counted(DevScene S, const float* __restrict__ rays,
@@ -202,22 +220,45 @@ int df_grid(spt_context* ctx) {
     return grid;
 }
 
-// The persistent closest-hit launch.
+// The persistent closest-hit launch (in the order `order` when it is not NULL, the hits then in that
+// order; the ordered kernel has the plain one's registers and block, so the same grid).
 template <int STRIDE>
 spt_status launch_df(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
-                     unsigned long long* next, cudaStream_t s) {
-    k_intersect_df<STRIDE><<<df_grid<STRIDE>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status, next);
+                     unsigned long long* next, cudaStream_t s, const uint32_t* order = nullptr) {
+    if (order)
+        k_intersect_df_ordered<STRIDE>
+            <<<df_grid<STRIDE>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, order, n, d_hits, ctx->d_status, next);
+    else
+        k_intersect_df<STRIDE><<<df_grid<STRIDE>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status, next);
     SPT_CUDA(ctx, cudaGetLastError());
     return SPT_OK;
 }
 
 template <int STRIDE>
 spt_status launch_intersect_t(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
-                              cudaStream_t s) {
+                              cudaStream_t s, bool order) {
     if (sc->dev.traversal == 2) {
         unsigned long long* next = nullptr;
         spt_status st = fetch_counter(ctx, s, &next);
         if (st != SPT_OK) return st;
+        if (order && n >= order_min_rays() && n <= 0xFFFFFFFFull) {
+            // this stream's buffers: the hits in the order first (16-byte aligned for the kernel's
+            // float4 stores whatever n is), then the keys (n words), the order, its inverse and the
+            // traced count (2n + 1), and the sort's counts
+            const size_t work = order_scratch_bytes(ctx);
+            void* mem = nullptr;
+            if ((st = stream_scratch(ctx, s, (7 * n + 1) * sizeof(uint32_t) + work, &mem)) != SPT_OK) return st;
+            if (mem) {
+                spt_hit* ordered = static_cast<spt_hit*>(mem);
+                uint32_t* keys = reinterpret_cast<uint32_t*>(ordered + n);
+                uint32_t* ord = keys + n;
+                uint32_t* w = keys + 3 * n + 1;
+                if ((st = order_rays(ctx, sc, d_rays, n, STRIDE, s, keys, w, ord)) != SPT_OK) return st;
+                if ((st = launch_df<STRIDE>(ctx, sc, d_rays, n, ordered, next, s, ord)) != SPT_OK) return st;
+                return unorder_hits(ctx, ordered, ord, n, d_hits, s);
+            }
+            // every per-stream buffer belongs to another stream: the batch's own order
+        }
         return launch_df<STRIDE>(ctx, sc, d_rays, n, d_hits, next, s);
     } else if (sc->dev.traversal == 1) {
         k_intersect<1, STRIDE><<<blocks_for(n, kBlock), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status);
@@ -231,11 +272,11 @@ spt_status launch_intersect_t(spt_context* ctx, const spt_scene* sc, const float
 }  // namespace
 
 spt_status launch_intersect(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
-                            cudaStream_t s, int stride) {
+                            cudaStream_t s, int stride, bool order) {
     if (n == 0) return SPT_OK;
     if (n > (1ull << 36)) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "too many rays in one call");
-    if (stride == 6) return launch_intersect_t<6>(ctx, sc, d_rays, n, d_hits, s);
-    return launch_intersect_t<8>(ctx, sc, d_rays, n, d_hits, s);
+    if (stride == 6) return launch_intersect_t<6>(ctx, sc, d_rays, n, d_hits, s, order);
+    return launch_intersect_t<8>(ctx, sc, d_rays, n, d_hits, s, order);
 }
 
 // launch_intersect with the persistent kernel's ray counter supplied by the caller (zeroed on stream s
@@ -336,7 +377,7 @@ spt_status intersect_pipelined(spt_context* ctx, const spt_scene* sc, const floa
         const uint64_t first = c * kPipeChunk, m = std::min(kPipeChunk, n - first);
         SPT_CUDA(ctx, cudaMemcpyAsync(d_rays, rays + static_cast<uint64_t>(stride) * first, m * ray_bytes,
                                       cudaMemcpyHostToDevice, s));
-        if ((st = launch_intersect(ctx, sc, d_rays, m, d_hits, s, stride)) != SPT_OK) return st;
+        if ((st = launch_intersect(ctx, sc, d_rays, m, d_hits, s, stride, true)) != SPT_OK) return st;
         if (tests || nhits)
             if ((st = launch_count(ctx, sc, d_rays, m, nullptr, tests ? d_tests : nullptr, nhits ? d_nh : nullptr,
                                    nullptr, s, stride)) != SPT_OK)
@@ -371,7 +412,7 @@ spt_status intersect_host(spt_context* ctx, const spt_scene* sc, const float* ra
     if (nhits && (st = scratch(ctx, 3, n * 4, &d_nh)) != SPT_OK) return st;
     SPT_CUDA(ctx, cudaMemcpyAsync(d_rays, rays, n * ray_bytes, cudaMemcpyHostToDevice, ctx->stream));
     if ((st = launch_intersect(ctx, sc, static_cast<float*>(d_rays), n, static_cast<spt_hit*>(d_hits), ctx->stream,
-                               stride)) != SPT_OK)
+                               stride, true)) != SPT_OK)
         return st;
     if (tests || nhits)
         if ((st = launch_count(ctx, sc, static_cast<float*>(d_rays), n, nullptr, static_cast<uint32_t*>(d_tests),
@@ -403,7 +444,43 @@ spt_status spt_intersect_packed(spt_context* ctx, const spt_scene* sc, const flo
 spt_status spt_intersect_device(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n,
                                 spt_hit* d_hits, void* stream) {
     if (!ctx || !sc || (n && (!d_rays || !d_hits))) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
-    return launch_intersect(ctx, sc, d_rays, n, d_hits, static_cast<cudaStream_t>(stream));
+    return launch_intersect(ctx, sc, d_rays, n, d_hits, static_cast<cudaStream_t>(stream), 8, true);
+}
+
+spt_status spt_ray_order_device(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n,
+                                uint32_t* d_order, void* stream) {
+    if (!ctx || !sc || (n && (!d_rays || !d_order))) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0) return SPT_OK;
+    if (n > 0xFFFFFFFFull) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "a ray order holds fewer than 2^32 rays");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    void* mem = nullptr;
+    spt_status st = stream_scratch(ctx, s, n * sizeof(uint32_t) + order_scratch_bytes(ctx), &mem);
+    if (st != SPT_OK) return st;
+    if (!mem) return fail(ctx, SPT_ERR_UNSUPPORTED, "ray order buffers are held by eight other streams");
+    uint32_t* keys = static_cast<uint32_t*>(mem);
+    return order_rays(ctx, sc, d_rays, n, 8, s, keys, keys + n, d_order);
+}
+
+spt_status spt_intersect_ordered_device(spt_context* ctx, const spt_scene* sc, const float* d_rays,
+                                        const uint32_t* d_order, uint64_t n, spt_hit* d_hits_ordered, void* stream) {
+    if (!ctx || !sc || (n && (!d_rays || !d_order || !d_hits_ordered)))
+        return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0) return SPT_OK;
+    if (n > 0xFFFFFFFFull) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "a ray order holds fewer than 2^32 rays");
+    if (sc->dev.traversal != 2) return fail(ctx, SPT_ERR_UNSUPPORTED, "ordered queries run on the 8-wide persistent traversal");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned long long* next = nullptr;
+    spt_status st = fetch_counter(ctx, s, &next);
+    if (st != SPT_OK) return st;
+    return launch_df<8>(ctx, sc, d_rays, n, d_hits_ordered, next, s, d_order);
+}
+
+spt_status spt_hits_unorder_device(spt_context* ctx, const uint32_t* d_order, uint64_t n, const spt_hit* d_hits_ordered,
+                                   spt_hit* d_hits, void* stream) {
+    if (!ctx || (n && (!d_order || !d_hits_ordered || !d_hits))) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (n == 0) return SPT_OK;
+    if (n > 0xFFFFFFFFull) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "a ray order holds fewer than 2^32 rays");
+    return unorder_hits(ctx, d_hits_ordered, d_order, n, d_hits, static_cast<cudaStream_t>(stream));
 }
 
 spt_status spt_traversal_work_device(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n,

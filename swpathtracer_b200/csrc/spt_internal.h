@@ -40,6 +40,12 @@ struct spt_context {
     int df_grid[2] = {0, 0};
     // device address of the static buffer of spt_intersect_noalloc (noalloc.cu), looked up on first use
     void* noalloc_scratch = nullptr;
+    // buffers of the ray ordering pass (ray_order.cu), one per stream that ran a large query, so
+    // that queries on different streams never share one
+    static constexpr int kStreamScratch = 8;
+    cudaStream_t sscratch_stream[kStreamScratch] = {};
+    void* sscratch[kStreamScratch] = {};
+    size_t sscratch_bytes[kStreamScratch] = {};
 };
 
 struct spt_scene {
@@ -69,6 +75,9 @@ spt_status cuda_fail(spt_context* ctx, cudaError_t e, const char* what);
 
 // Grows scratch slot `i` of the context to at least `bytes`.
 spt_status scratch(spt_context* ctx, int i, size_t bytes, void** out);
+// A buffer of at least `bytes` that only work on stream s uses; *out = NULL when every per-stream
+// buffer already belongs to another stream.
+spt_status stream_scratch(spt_context* ctx, cudaStream_t s, size_t bytes, void** out);
 spt_status pinned(spt_context* ctx, size_t bytes, void** out);
 
 // Reads the device status word and maps it to a status (resets it).
@@ -79,9 +88,21 @@ spt_status check_status(spt_context* ctx);
 spt_status make_camera(spt_context* ctx, const spt_camera* cam, DevCamera& out);
 
 // Kernel launchers (raycast.cu)
-// stride: floats per ray, 8 ({origin, pad, direction, pad}) or 6 (the reference's Ray, core/ray.h)
+// stride: floats per ray, 8 ({origin, pad, direction, pad}) or 6 (the reference's Ray, core/ray.h).
+// order: a batch of at least order_min_rays() rays on the persistent traversal is first put in
+// coherence order (order_rays); the hits are the same either way.
 spt_status launch_intersect(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
-                            cudaStream_t s, int stride = 8);
+                            cudaStream_t s, int stride = 8, bool order = false);
+// ray_order.cu: the coherence order of n < 2^32 device rays on stream s.  keys: n entries, work:
+// order_scratch_bytes(ctx) bytes, order: 2n + 1 entries (order[k] = the k-th ray to trace for k below
+// order[2n], the rays that meet the root box; order[n + i] = ray i's place, 0xFFFFFFFF for a ray that
+// misses).  unorder_hits: hits[i] = ordered[order[n + i]], or the miss record.
+uint64_t order_min_rays();
+size_t order_scratch_bytes(spt_context* ctx);
+spt_status order_rays(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, int stride,
+                      cudaStream_t s, uint32_t* keys, uint32_t* work, uint32_t* order);
+spt_status unorder_hits(spt_context* ctx, const spt_hit* ordered, const uint32_t* order, uint64_t n, spt_hit* hits,
+                        cudaStream_t s);
 spt_status launch_count(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_ref_hits,
                         uint32_t* d_tests, uint32_t* d_hits, uint32_t* d_prim_tests, cudaStream_t s, int stride = 8);
 

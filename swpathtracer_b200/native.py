@@ -29,6 +29,9 @@ PROTOTYPES = {
     "spt_intersect": (i32, [vp, vp, vp, u64, vp, vp, vp]),
     "spt_intersect_packed": (i32, [vp, vp, vp, u64, vp, vp, vp]),
     "spt_intersect_device": (i32, [vp, vp, vp, u64, vp, vp]),
+    "spt_ray_order_device": (i32, [vp, vp, vp, u64, vp, vp]),
+    "spt_intersect_ordered_device": (i32, [vp, vp, vp, vp, u64, vp, vp]),
+    "spt_hits_unorder_device": (i32, [vp, vp, u64, vp, vp, vp]),
     "spt_count_device": (i32, [vp, vp, vp, u64, vp, vp, vp, vp, vp]),
     "spt_traversal_work_device": (i32, [vp, vp, vp, u64, vp, vp]),
     "spt_intersect_noalloc": (i32, [vp, vp, vp, u64, vp, vp, vp]),

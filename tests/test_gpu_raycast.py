@@ -145,6 +145,56 @@ def test_pipelined_host_queries_match_device_queries(device):
     np.testing.assert_array_equal(a["nhits"], b["nhits"])
 
 
+def test_coherence_order_keeps_every_hit(device):
+    """A batch of at least 2^21 rays is traced in coherence order (entry point into the root box, then
+    direction; misses last) and its hits go back to each ray's own index.  Against the same rays in
+    calls below that size (their own order), bit for bit, on a batch whose keys reach every edge:
+    axis-aligned directions (zero components), origins inside the root box, rays that miss it, and
+    both ray layouts."""
+    import torch
+    packed = scenes.displaced_mesh_scene(6).build()
+    gs = spt.GpuScene(device, packed)
+    n = (1 << 21) + 17
+    rays = scenes.incoherent_rays(n, seed=79, half_extent=1.5)
+    axes = np.eye(3, dtype=np.float32)
+    k = np.arange(60000)
+    rays[k, 4:7] = axes[k % 3] * np.where(k % 2, 1.0, -1.0)[:, None]       # axis-aligned directions
+    rays[60000:90000, 0:3] *= 0.3                                           # origins inside the box
+    d_rays = torch.from_numpy(rays).cuda()
+    ordered = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    plain = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    gs.intersect_device(d_rays.data_ptr(), n, ordered.data_ptr(), 0)
+    half = n // 2                                                           # both calls below 2^21
+    gs.intersect_device(d_rays.data_ptr(), half, plain.data_ptr(), 0)
+    gs.intersect_device(d_rays[half:].data_ptr(), n - half, plain[half:].data_ptr(), 0)
+    torch.cuda.synchronize()
+    assert torch.equal(ordered, plain)
+    # the three stages one by one: the order is a permutation with its inverse, and the hits in that
+    # order are the rays' hits
+    order = torch.empty(2 * n + 1, dtype=torch.int32, device="cuda")
+    in_order = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    back = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    gs.ray_order_device(d_rays.data_ptr(), n, order.data_ptr(), 0)
+    gs.intersect_ordered_device(d_rays.data_ptr(), order.data_ptr(), n, in_order.data_ptr(), 0)
+    gs.hits_unorder_device(order.data_ptr(), n, in_order.data_ptr(), back.data_ptr(), 0)
+    torch.cuda.synchronize()
+    m = int(order[2 * n].item())
+    perm = order[:m].long()
+    inv = order[n:2 * n]
+    placed = inv != -1                                   # 0xFFFFFFFF: the root box test rejects the ray
+    assert int(placed.sum().item()) == m
+    idx = torch.arange(n, device="cuda")
+    assert torch.equal(torch.sort(perm).values, idx[placed])
+    assert torch.equal(perm[inv[placed].long()], idx[placed])
+    assert torch.equal(in_order[:m], plain[perm]) and torch.equal(back, plain)
+    assert (plain[~placed][:, 1] == -1).all()            # every ray without a place misses
+    miss = ordered[:, 1].cpu().numpy().view(np.uint32) == abi.SPT_MISS
+    assert 0.2 < miss.mean() < 0.9
+    # the reference's 24-byte layout through the pageable path, ordered as well
+    rays6 = np.ascontiguousarray(np.concatenate([rays[:, 0:3], rays[:, 4:7]], axis=1))
+    assert gs.intersect(rays6)["hits"].tobytes() == ordered.cpu().numpy().tobytes()
+
+
 def test_reference_ray_layout_matches_padded_layout(device):
     """spt_intersect_packed takes rays as the reference's Ray lies in memory (origin then direction,
     24 bytes): the same hits and counts as the padded layout, on the pageable path, the pipelined
