@@ -466,7 +466,7 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            prof = json.load(f).get("k_intersect_df") or {}
+            prof = json.load(f).get("k_intersect_df_ordered") or {}
         if prof:
             traffic = prof["bytes_per_ray"] * n
     # the kernel's own work on a sample of the same rays (an extra, untimed launch with counters)

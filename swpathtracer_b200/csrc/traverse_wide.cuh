@@ -320,10 +320,13 @@ struct WideTraversalT {
 // Persistent warps with dynamic ray fetch (after Aila & Laine, "Understanding the Efficiency of Ray
 // Traversal on GPUs", HPG 2009): a lane whose ray is finished takes the next ray at once instead of
 // idling until the warp's longest ray ends.  Ray indices come from a warp-local pool refilled
-// kChunk at a time from one global counter, so the counter sees one atomic per kChunk rays (64:
-// measured 1.5 % faster than 256 on the incoherent workload, from a shorter tail).
+// kChunk at a time from one global counter, so the counter sees one atomic per kChunk rays.  32 is
+// the least that works (one refill may hand up to 32 lanes rays from a fresh chunk): against 64 it
+// measured +0.6 % on the ordered incoherent queries and +4.6 % / +8.2 % on the box and layered path
+// tracing (a shorter tail, and the ordered neighbours stay together); 128 lost 3 %.
 // load(i, o, d) fetches ray i; store(i, h) writes its result.
-constexpr uint32_t kChunk = 64;
+constexpr uint32_t kChunk = 32;
+static_assert(kChunk >= 32, "a refill takes up to 32 rays from one fresh chunk");
 // Refill once this many lanes wait for a ray (or no lane is busy): the refill branch runs with only
 // the waiting lanes, so batching it pays a little (2,674 -> 2,690 Mrays/s at 4; 2 and 8 gain less).
 constexpr int kRefill = 4;
