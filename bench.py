@@ -229,6 +229,18 @@ def guided_c4(spt, scenes, dev, torch, spp=1024, ref_spp=2048, batch=1 << 18, st
         g = spt.Guide(dev, spt.guide_config(batch=batch, max_steps=steps, mix=mix, seed=7 + i, guided_depth=depth))
         guided, tg = render(spp, 7 + i, g)
         g.close()
+        if tp < 0.5:
+            # a render of tens of milliseconds is timed three times per arm (the same work: the same
+            # seeds, a fresh guide each time) and the median kept, so that one host hiccup does not
+            # decide the scene; the images of the first renders are the ones compared
+            tps, tgs = [tp], [tg]
+            for _ in range(2):
+                tps.append(render(spp, 7 + i)[1])
+                g = spt.Guide(dev, spt.guide_config(batch=batch, max_steps=steps, mix=mix, seed=7 + i,
+                                                    guided_depth=depth))
+                tgs.append(render(spp, 7 + i, g)[1])
+                g.close()
+            tp, tg = sorted(tps)[1], sorted(tgs)[1]
         gs.close()
         nonfinite += int((~torch.isfinite(guided)).sum().item())
         ep, eg = relmse(plain, ref), relmse(guided, ref)
@@ -244,6 +256,7 @@ def guided_c4(spt, scenes, dev, torch, spp=1024, ref_spp=2048, batch=1 << 18, st
            key + "_equal_time_relmse_ratio_debiased": round(spd / max(sgd, 1e-30), 4),
            key + "_geomean_per_scene_ratio": round(math.exp(sum(math.log(x) for x in per) / len(per)), 4),
            key + "_per_scene_ratios": [round(x, 3) for x in per],
+           key + "_per_scene_ms_plain_guided": [[round(1e3 * r[3], 1), round(1e3 * r[4], 1)] for r in rows],
            key + "_wall_s_plain": round(sum(r[3] for r in rows), 3),
            key + "_wall_s_guided": round(sum(r[4] for r in rows), 3),
            key + "_reference_spp": ref_spp, key + "_nonfinite_pixels": nonfinite,

@@ -195,6 +195,43 @@ def test_coherence_order_keeps_every_hit(device):
     assert gs.intersect(rays6)["hits"].tobytes() == ordered.cpu().numpy().tobytes()
 
 
+def test_coherence_order_on_spheres_and_unsupported_scenes(device, oracle):
+    """The ordered path on a sphere scene (the 8-wide tree's sphere leaves) equals the oracle on a
+    sample and the batch's own order everywhere; a scene without the persistent traversal (no
+    acceleration structure) keeps its own order in spt_intersect_device and refuses the ordered
+    stage with SPT_ERR_UNSUPPORTED."""
+    import torch
+    from swpathtracer_b200.native import SptError
+    packed = scenes.furnace_scene("coating").build()
+    gs = spt.GpuScene(device, packed)
+    n = (1 << 21) + 5
+    rays = scenes.incoherent_rays(n, seed=80, half_extent=12.0)
+    d_rays = torch.from_numpy(rays).cuda()
+    ordered = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    plain = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    gs.intersect_device(d_rays.data_ptr(), n, ordered.data_ptr(), 0)
+    half = n // 2
+    gs.intersect_device(d_rays.data_ptr(), half, plain.data_ptr(), 0)
+    gs.intersect_device(d_rays[half:].data_ptr(), n - half, plain[half:].data_ptr(), 0)
+    torch.cuda.synchronize()
+    assert torch.equal(ordered, plain)
+    exp = oracle.scene(packed).intersect(rays[:20000])
+    got = ordered[:20000].cpu().numpy()
+    np.testing.assert_array_equal(got[:, 1].view(np.uint32), exp["hits"]["prim_id"])
+    sb = scenes.box_scene(2)
+    sb.accel = abi.ACCEL_NONE
+    flat = spt.GpuScene(device, sb.build())
+    order = torch.empty(2 * n + 1, dtype=torch.int32, device="cuda")
+    flat.ray_order_device(d_rays.data_ptr(), n, order.data_ptr(), 0)      # the order itself is defined
+    with pytest.raises(SptError):
+        flat.intersect_ordered_device(d_rays.data_ptr(), order.data_ptr(), n, ordered.data_ptr(), 0)
+    m = 50000
+    flat.intersect_device(d_rays.data_ptr(), m, plain.data_ptr(), 0)
+    torch.cuda.synchronize()
+    exp = oracle.scene(sb.build()).intersect(rays[:m])
+    np.testing.assert_array_equal(plain[:m, 1].cpu().numpy().view(np.uint32), exp["hits"]["prim_id"])
+
+
 def test_reference_ray_layout_matches_padded_layout(device):
     """spt_intersect_packed takes rays as the reference's Ray lies in memory (origin then direction,
     24 bytes): the same hits and counts as the padded layout, on the pageable path, the pipelined
