@@ -49,6 +49,12 @@ def args_():
     p.add_argument("--c4-steps", type=int, default=256)
     p.add_argument("--c4-mix", type=float, default=0.5)
     p.add_argument("--c4-depth", type=int, default=0, help="guided_depth of the C4 guides (0: every vertex)")
+    p.add_argument("--pt-only", action="store_true",
+                   help="only the C0 and C2 path-tracing measurements (one JSON line)")
+    p.add_argument("--pt-renders", type=int, default=7, help="timed renders per workload (the median is kept)")
+    p.add_argument("--pt-workload", choices=["both", "box", "layered"], default="both")
+    p.add_argument("--pt-host-loop", action="store_true",
+                   help="path tracing with the host-driven loop (profilers cannot see into the device loop)")
     p.add_argument("--guide-train-only", action="store_true",
                    help="only the guide's training-step times on 2^18 device records (one JSON line)")
     return p.parse_args()
@@ -180,6 +186,42 @@ def guided_vs_plain(spt, scenes, dev, torch, name, sb, spp, ref_spp, steps, seed
     return {name + "_spp": spp, name + "_relmse_plain": round(ep / k, 6), name + "_relmse_guided": round(eg / k, 6),
             name + "_wall_ms_plain": round(1e3 * tp / k, 2), name + "_wall_ms_guided": round(1e3 * tg / k, 2),
             name + "_equal_time_relmse_ratio_plain_over_guided": round((ep * tp) / (eg * tg), 4)}
+
+
+def path_tracing(spt, scenes, dev, torch, subdiv, renders=7, workload="both", host_loop=False):
+    """Path tracing of C0 (box, 256^2, 16 spp, max length 5) and C2 (the layered mesh in the box x3,
+    800 x 600, RR after 3, cap 16; 16 spp: the throughput does not depend on spp), each the median of
+    `renders` device-timed renders (spt_pathtrace_device: one launch of the render's graph).  With
+    host_loop, the same render as a one-job batch whose loop the host drives (tune.host_loop: a graph
+    of two iterations replayed from the host, which kernel profilers can see into)."""
+    from swpathtracer_b200 import abi
+    extras = {}
+    tune = abi.Tune(capacity=1 << 21, extend_block=128, shade_block=128, traversal=-1, check_every=8, host_loop=1)
+    for key, sb, cam, prm in (
+            ("pt_box_256x256_16spp", scenes.box_scene(5), scenes.box_camera(256, 256),
+             scenes.pt_params(spp=16, sampler="jittered", termination="max-length", path_length=5, seed=3)),
+            ("pt_layered_800x600_rr3_max16", scenes.layered_box_scene(subdiv), scenes.layered_box_camera(800, 600),
+             scenes.pt_params(spp=16, sampler="jittered", termination="russian-roulette", path_length=3,
+                              max_depth=16, seed=4))):
+        if workload != "both" and not key.startswith("pt_" + workload):
+            continue
+        pgs = spt.GpuScene(dev, sb.build())
+        img = torch.empty(cam.width * cam.height * 3, dtype=torch.float32, device="cuda")
+        if host_loop:
+            one = lambda: spt.render_batch(dev, [(pgs, cam, prm)], [img.data_ptr()], tune=tune)[0]
+        else:
+            one = lambda: pgs.pathtrace_device(cam, prm, img.data_ptr())
+        for _ in range(2):
+            one()
+        # renders of a few ms each; the median is robust to a transient on a shared machine
+        runs = sorted((one() for _ in range(renders)), key=lambda r: r.gpu_ms)
+        mid = runs[len(runs) // 2]
+        paths, segs, ms = mid.paths, mid.segments, mid.gpu_ms
+        extras[key + "_Mpaths_s"] = round(paths / (ms / 1e3) / 1e6, 3)
+        extras[key + "_Mrays_s"] = round(segs / (ms / 1e3) / 1e6, 2)
+        extras[key + "_segments_per_path"] = round(segs / paths, 3)
+        pgs.close()
+    return extras
 
 
 def guided_c4(spt, scenes, dev, torch, spp=1024, ref_spp=2048, batch=1 << 18, steps=256, mix=0.5, depth=0, n=64):
@@ -380,6 +422,12 @@ def main():
         print(json.dumps(guide_train_steps(spt, abi, dev, torch)), flush=True)
         dev.close()
         return
+    if a.pt_only:
+        dev = spt.Device(local)
+        print(json.dumps(path_tracing(spt, scenes, dev, torch, a.subdiv, renders=a.pt_renders, workload=a.pt_workload,
+                                      host_loop=a.pt_host_loop)), flush=True)
+        dev.close()
+        return
     if a.c4_only:
         dev = spt.Device(local)
         print(json.dumps(guided_c4(spt, scenes, dev, torch, spp=a.c4_spp, ref_spp=a.c4_ref_spp, steps=a.c4_steps,
@@ -554,24 +602,7 @@ def main():
         dbvh.close()
         # path tracing: the CPU-runnable box scene (20,492 tris, 256x256, 16 spp, max length 5) and the
         # 1.3M-tri layered scene (800x600, russian roulette after 3, max depth 16), Mpaths/s
-        for key, sb, cam, prm in (
-                ("pt_box_256x256_16spp", scenes.box_scene(5), scenes.box_camera(256, 256),
-                 scenes.pt_params(spp=16, sampler="jittered", termination="max-length", path_length=5, seed=3)),
-                ("pt_layered_800x600_rr3_max16", scenes.layered_box_scene(a.subdiv), scenes.layered_box_camera(800, 600),
-                 scenes.pt_params(spp=16, sampler="jittered", termination="russian-roulette", path_length=3,
-                                  max_depth=16, seed=4))):
-            pgs = spt.GpuScene(dev, sb.build())
-            img = torch.empty(cam.width * cam.height * 3, dtype=torch.float32, device="cuda")
-            for _ in range(2):
-                pgs.pathtrace_device(cam, prm, img.data_ptr())
-            # seven renders of a few ms each; the median is robust to a transient on a shared machine
-            runs = sorted((pgs.pathtrace_device(cam, prm, img.data_ptr()) for _ in range(7)), key=lambda r: r.gpu_ms)
-            mid = runs[len(runs) // 2]
-            paths, segs, ms = mid.paths, mid.segments, mid.gpu_ms
-            extras[key + "_Mpaths_s"] = round(paths / (ms / 1e3) / 1e6, 3)
-            extras[key + "_Mrays_s"] = round(segs / (ms / 1e3) / 1e6, 2)
-            extras[key + "_segments_per_path"] = round(segs / paths, 3)
-            pgs.close()
+        extras.update(path_tracing(spt, scenes, dev, torch, a.subdiv))
         # batched uneven scenes: 64 seeded scenes (1k-500k tris, 128^2-1024^2, 64 spp) in one wavefront,
         # settings from the autotuner (its trials are not timed)
         batch = scenes.batched_scenes()

@@ -295,7 +295,10 @@ typedef struct spt_tune {
                                more ends the render with SPT_ERR_OVERFLOW */
     uint32_t max_iterations;/* wavefront iterations before the render gives up with SPT_ERR_TIMEOUT;
                                0 = a bound from the path count and the 1000-bounce roulette cap */
-    uint32_t reserved;      /* must be 0 */
+    uint32_t host_loop;     /* 1: the host replays a graph of two wavefront iterations and reads the
+                               counters every check_every iterations (the loop guided training uses)
+                               instead of the device-side WHILE loop; for tools that cannot look into
+                               graphs with conditional nodes, such as kernel profilers.  0 = default */
 } spt_tune;
 
 typedef struct spt_batch_job {

@@ -99,7 +99,7 @@ class Tune(C.Structure):
     _fields_ = [("capacity", C.c_uint32), ("extend_block", C.c_uint32), ("shade_block", C.c_uint32),
                 ("traversal", C.c_int32), ("check_every", C.c_uint32), ("sort_shading", C.c_uint32),
                 ("stack", C.c_uint32), ("stack_limit", C.c_uint32), ("max_iterations", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("host_loop", C.c_uint32)]
 
 
 class BatchJob(C.Structure):

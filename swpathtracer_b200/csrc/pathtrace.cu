@@ -688,9 +688,10 @@ spt_status render_jobs(spt_context* ctx, std::vector<PtJob>& jobs, const spt_tun
     uint64_t max_iter = std::min<uint64_t>((total / cap + 2) * 1100ull, 0xFFFFFFF0ull);
     if (tune.max_iterations) max_iter = std::min<uint64_t>(max_iter, tune.max_iterations);
     // Only a guide that trains during the render needs the host between iterations (it runs the
-    // optimiser steps on the records the paths wrote).  Every other render is one launch of a graph
-    // whose WHILE node repeats two iterations until k_continue sees the pool drained.
-    const bool host_loop = guide && train_budget > 0;
+    // optimiser steps on the records the paths wrote), or a caller that asks for the host-driven loop
+    // (tune.host_loop).  Every other render is one launch of a graph whose WHILE node repeats two
+    // iterations until k_continue sees the pool drained.
+    const bool host_loop = (guide && train_budget > 0) || tune.host_loop != 0;
     auto record_iterations = [&](cudaGraphConditionalHandle* loop) {
         for (int it = 0; it < 2; ++it) {
             PathBuf& cur = it ? B : A;
