@@ -237,7 +237,9 @@ spt_status spt_intersect_device(spt_context* ctx, const spt_scene* scene, const 
 spt_status spt_ray_order_device(spt_context* ctx, const spt_scene* scene, const float* d_rays, uint64_t n,
                                 uint32_t* d_order, void* stream);
 /* 2. Closest hits of the rays d_rays[d_order[k]] into d_hits_ordered[k], k < d_order[2n], on the
- *    persistent 8-wide traversal (SPT_ERR_UNSUPPORTED for a scene on another traversal). */
+ *    persistent 8-wide traversal (SPT_ERR_UNSUPPORTED for a scene on another traversal).  d_order
+ *    must come from stage 1 for the same rays and the same scene: a ray it leaves out is taken to
+ *    miss that scene's root box. */
 spt_status spt_intersect_ordered_device(spt_context* ctx, const spt_scene* scene, const float* d_rays,
                                         const uint32_t* d_order, uint64_t n, spt_hit* d_hits_ordered,
                                         void* stream);
