@@ -461,10 +461,11 @@ def main():
 
     # A step is spt_intersect_device's three stages called one by one, so that the traversal kernel's
     # own time can be bracketed by events inside the timed region: the coherence order of the batch
-    # (four kernels: per-block key histograms, their offsets, the scan of the key totals, the
-    # scatter), the persistent closest-hit kernel in that order, and the gather of the hits back to
-    # the rays' own indices.  All of it runs on the legacy default stream, torch's current stream
-    # here, so the events see the kernels.
+    # (three kernels: per-block key histograms, their per-key offsets, the scan of the key totals
+    # with the scatter), the persistent closest-hit kernel in that order (after a one-thread kernel
+    # that holds the order's traced count to the batch), and the gather of the hits back to the rays'
+    # own indices.  All of it runs on the legacy default stream, torch's current stream here, so the
+    # events see the kernels.
     d_order = torch.empty(2 * n + 1, dtype=torch.int32, device="cuda")
     d_hits_ordered = torch.empty((n, 4), dtype=torch.int32, device="cuda")
     kernels_per_step = 6

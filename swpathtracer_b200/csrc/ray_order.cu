@@ -226,8 +226,9 @@ __global__ void __launch_bounds__(kOrderThreads) k_order_scatter(const uint32_t*
     }
 }
 
-// hits[i] = ordered[inverse[i]]: the hits back at the rays' own places; a ray with no place gets the
-// record the traversal writes for a ray its root test rejects (t = +inf, SPT_MISS, u = v = 0).
+// hits[i] = ordered[inverse[i]]: the hits back at the rays' own places; a ray with no place (kMiss,
+// or any place outside the batch) gets the record the traversal writes for a ray its root test
+// rejects (t = +inf, SPT_MISS, u = v = 0).
 __global__ void __launch_bounds__(256) k_order_gather(const spt_hit* __restrict__ ordered,
                                                       const uint32_t* __restrict__ inverse, uint32_t n,
                                                       spt_hit* __restrict__ hits) {
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(256) k_order_gather(const spt_hit* __restrict_
             const uint64_t i = base + static_cast<uint64_t>(j) * stride;
             if (i < n) {
                 const uint32_t p = __ldg(inverse + i);
-                h[j] = p != kMiss ? __ldg(reinterpret_cast<const float4*>(ordered) + p)
+                h[j] = p < n ? __ldg(reinterpret_cast<const float4*>(ordered) + p)
                                   : make_float4(__int_as_float(0x7f800000), __uint_as_float(SPT_MISS), 0.0f, 0.0f);
             }
         }

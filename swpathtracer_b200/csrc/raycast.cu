@@ -52,15 +52,16 @@ __global__ void __launch_bounds__(kBlock, 10) k_intersect_df(DevScene S, const f
 }
 
 // The same kernel over a batch in coherence order (ray_order.cu): the k-th ray it takes is order[k],
-// for k below order[2n] (the rays that meet the root box), and its hit goes to place k of
-// hits_ordered, so that neighbouring lanes write neighbouring hits (scattered 16-byte stores cost
-// partial-sector writes in DRAM).
+// for k below *count (the rays that meet the root box), and its hit goes to place k of hits_ordered,
+// so that neighbouring lanes write neighbouring hits (scattered 16-byte stores cost partial-sector
+// writes in DRAM).
 template <int STRIDE>
 __global__ void __launch_bounds__(kBlock, 10) k_intersect_df_ordered(DevScene S, const float* __restrict__ rays,
-                                                                 const uint32_t* __restrict__ order, uint64_t n,
+                                                                 const uint32_t* __restrict__ order,
+                                                                 const uint32_t* __restrict__ count,
                                                                  spt_hit* __restrict__ hits_ordered, uint32_t* status,
                                                                  unsigned long long* next) {
-    const uint64_t traced = __ldg(order + 2 * n);
+    const uint64_t traced = __ldg(count);
     persistent_trace(
         S, traced, next, status, [&](uint64_t k, V3& o, V3& d) { load_ray<STRIDE, true>(rays, __ldg(order + k), o, d); },
         [&](uint64_t k, const Hit1& h) {
@@ -220,14 +221,23 @@ int df_grid(spt_context* ctx) {
     return grid;
 }
 
-// The persistent closest-hit launch (in the order `order` when it is not NULL, the hits then in that
-// order; the ordered kernel has the plain one's registers and block, so the same grid).
+// A caller's traced count held to the batch: *out = min(order[2n], n), so that an order made for
+// another batch cannot take the traversal past this one's order entries and hit slots.
+__global__ void k_order_count_clamp(const uint32_t* __restrict__ order, uint64_t n, uint32_t* __restrict__ out) {
+    const uint32_t c = order[2 * n];
+    *out = c < n ? c : static_cast<uint32_t>(n);
+}
+
+// The persistent closest-hit launch (in the order `order` when it is not NULL, over the count at
+// `count`, the hits then in that order; the ordered kernel has the plain one's registers and block,
+// so the same grid).
 template <int STRIDE>
 spt_status launch_df(spt_context* ctx, const spt_scene* sc, const float* d_rays, uint64_t n, spt_hit* d_hits,
-                     unsigned long long* next, cudaStream_t s, const uint32_t* order = nullptr) {
+                     unsigned long long* next, cudaStream_t s, const uint32_t* order = nullptr,
+                     const uint32_t* count = nullptr) {
     if (order)
         k_intersect_df_ordered<STRIDE>
-            <<<df_grid<STRIDE>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, order, n, d_hits, ctx->d_status, next);
+            <<<df_grid<STRIDE>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, order, count, d_hits, ctx->d_status, next);
     else
         k_intersect_df<STRIDE><<<df_grid<STRIDE>(ctx), kBlock, 0, s>>>(sc->dev, d_rays, n, d_hits, ctx->d_status, next);
     SPT_CUDA(ctx, cudaGetLastError());
@@ -254,7 +264,7 @@ spt_status launch_intersect_t(spt_context* ctx, const spt_scene* sc, const float
                 uint32_t* ord = keys + n;
                 uint32_t* w = keys + 3 * n + 1;
                 if ((st = order_rays(ctx, sc, d_rays, n, STRIDE, s, keys, w, ord)) != SPT_OK) return st;
-                if ((st = launch_df<STRIDE>(ctx, sc, d_rays, n, ordered, next, s, ord)) != SPT_OK) return st;
+                if ((st = launch_df<STRIDE>(ctx, sc, d_rays, n, ordered, next, s, ord, ord + 2 * n)) != SPT_OK) return st;
                 return unorder_hits(ctx, ordered, ord, n, d_hits, s);
             }
             // every per-stream buffer belongs to another stream: the batch's own order
@@ -472,7 +482,13 @@ spt_status spt_intersect_ordered_device(spt_context* ctx, const spt_scene* sc, c
     unsigned long long* next = nullptr;
     spt_status st = fetch_counter(ctx, s, &next);
     if (st != SPT_OK) return st;
-    return launch_df<8>(ctx, sc, d_rays, n, d_hits_ordered, next, s, d_order);
+    // a second slot of the counter ring holds the clamped count for this call
+    unsigned long long* count_slot = nullptr;
+    if ((st = fetch_counter(ctx, s, &count_slot)) != SPT_OK) return st;
+    uint32_t* count = reinterpret_cast<uint32_t*>(count_slot);
+    k_order_count_clamp<<<1, 1, 0, s>>>(d_order, n, count);
+    SPT_CUDA(ctx, cudaGetLastError());
+    return launch_df<8>(ctx, sc, d_rays, n, d_hits_ordered, next, s, d_order, count);
 }
 
 spt_status spt_hits_unorder_device(spt_context* ctx, const uint32_t* d_order, uint64_t n, const spt_hit* d_hits_ordered,
