@@ -180,7 +180,10 @@ typedef struct spt_bvh spt_bvh;
 /* ---- library / context --------------------------------------------------------------- */
 uint32_t spt_abi_version(void);
 /* Creates a context on CUDA device `device` (Integrator/Scene owner; reference
- * core/swpathtracer_app.cpp:29-37 plays this role on the CPU). */
+ * core/swpathtracer_app.cpp:29-37 plays this role on the CPU).  A context serves one host thread at
+ * a time: its scratch buffers, per-stream buffers and counter ring are not locked, so host threads
+ * that call concurrently take a context each (or serialise their calls).  Device work that one
+ * thread queues on different streams of a context may overlap. */
 spt_status spt_create(int device, spt_context** out);
 spt_status spt_destroy(spt_context* ctx);
 /* Text of the last error on this context (never NULL). */
