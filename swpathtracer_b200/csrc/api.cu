@@ -70,9 +70,16 @@ spt_status pinned(spt_context* ctx, size_t bytes, void** out) {
     return SPT_OK;
 }
 
-spt_status fetch_counter(spt_context* ctx, cudaStream_t s, unsigned long long** out) {
+spt_status ring_slot(spt_context* ctx, unsigned long long** out) {
     if (!ctx->d_fetch) SPT_CUDA(ctx, cudaMalloc(&ctx->d_fetch, kFetchRing * sizeof(unsigned long long)));
-    unsigned long long* c = ctx->d_fetch + (ctx->fetch_slot++ % kFetchRing);
+    *out = ctx->d_fetch + (ctx->fetch_slot++ % kFetchRing);
+    return SPT_OK;
+}
+
+spt_status fetch_counter(spt_context* ctx, cudaStream_t s, unsigned long long** out) {
+    unsigned long long* c = nullptr;
+    spt_status st = ring_slot(ctx, &c);
+    if (st != SPT_OK) return st;
     SPT_CUDA(ctx, cudaMemsetAsync(c, 0, sizeof(unsigned long long), s));
     *out = c;
     return SPT_OK;

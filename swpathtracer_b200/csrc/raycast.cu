@@ -222,10 +222,13 @@ int df_grid(spt_context* ctx) {
 }
 
 // A caller's traced count held to the batch: *out = min(order[2n], n), so that an order made for
-// another batch cannot take the traversal past this one's order entries and hit slots.
-__global__ void k_order_count_clamp(const uint32_t* __restrict__ order, uint64_t n, uint32_t* __restrict__ out) {
+// another batch cannot take the traversal past this one's order entries and hit slots; and the
+// persistent kernel's ray counter zeroed, in the same one-thread launch.
+__global__ void k_order_count_clamp(const uint32_t* __restrict__ order, uint64_t n, uint32_t* __restrict__ out,
+                                    unsigned long long* __restrict__ next) {
     const uint32_t c = order[2 * n];
     *out = c < n ? c : static_cast<uint32_t>(n);
+    *next = 0ull;
 }
 
 // The persistent closest-hit launch (in the order `order` when it is not NULL, over the count at
@@ -479,14 +482,13 @@ spt_status spt_intersect_ordered_device(spt_context* ctx, const spt_scene* sc, c
     if (n > 0xFFFFFFFFull) return fail(ctx, SPT_ERR_INVALID_ARGUMENT, "a ray order holds fewer than 2^32 rays");
     if (sc->dev.traversal != 2) return fail(ctx, SPT_ERR_UNSUPPORTED, "ordered queries run on the 8-wide persistent traversal");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    unsigned long long* next = nullptr;
-    spt_status st = fetch_counter(ctx, s, &next);
+    // two slots of the counter ring: the ray counter and the clamped count, both set by one kernel
+    unsigned long long *next = nullptr, *count_slot = nullptr;
+    spt_status st = ring_slot(ctx, &next);
     if (st != SPT_OK) return st;
-    // a second slot of the counter ring holds the clamped count for this call
-    unsigned long long* count_slot = nullptr;
-    if ((st = fetch_counter(ctx, s, &count_slot)) != SPT_OK) return st;
+    if ((st = ring_slot(ctx, &count_slot)) != SPT_OK) return st;
     uint32_t* count = reinterpret_cast<uint32_t*>(count_slot);
-    k_order_count_clamp<<<1, 1, 0, s>>>(d_order, n, count);
+    k_order_count_clamp<<<1, 1, 0, s>>>(d_order, n, count, next);
     SPT_CUDA(ctx, cudaGetLastError());
     return launch_df<8>(ctx, sc, d_rays, n, d_hits_ordered, next, s, d_order, count);
 }

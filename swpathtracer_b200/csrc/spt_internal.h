@@ -111,6 +111,8 @@ constexpr uint32_t kFetchRing = 1024;
 
 // Zeroes the next counter of the ring on stream s and returns it (persistent kernels).
 spt_status fetch_counter(spt_context* ctx, cudaStream_t s, unsigned long long** out);
+// The next slot of the ring as it is (the caller's kernel initialises it).
+spt_status ring_slot(spt_context* ctx, unsigned long long** out);
 // Blocks of `block` threads that fill every SM once for `kernel` (persistent launches).
 int persistent_grid(spt_context* ctx, const void* kernel, int block);
 
