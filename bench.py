@@ -175,12 +175,24 @@ def guided_vs_plain(spt, scenes, dev, torch, name, sb, spp, ref_spp, steps, seed
     ep = eg = tp = tg = 0.0
     for seed in seeds:
         plain, t = render(spp, seed)
-        ep, tp = ep + relmse(plain, ref), tp + t
         g = spt.Guide(dev, spt.guide_config(batch=1 << 16, max_steps=steps, mix=mix, seed=seed,
                                                  cache_res=cache_res))
-        guided, t = render(spp, seed, g)
-        eg, tg = eg + relmse(guided, ref), tg + t
+        guided, u = render(spp, seed, g)
         g.close()
+        if t < 0.2:
+            # renders of about 100 ms are timed three times per arm (the same work, a fresh guide each
+            # time) and the median kept: the guided arm's training loop waits on the host, so one
+            # stretch of host contention would otherwise decide the line
+            ts, us = [t], [u]
+            for _ in range(2):
+                ts.append(render(spp, seed)[1])
+                g = spt.Guide(dev, spt.guide_config(batch=1 << 16, max_steps=steps, mix=mix, seed=seed,
+                                                         cache_res=cache_res))
+                us.append(render(spp, seed, g)[1])
+                g.close()
+            t, u = sorted(ts)[1], sorted(us)[1]
+        ep, tp = ep + relmse(plain, ref), tp + t
+        eg, tg = eg + relmse(guided, ref), tg + u
     gs.close()
     k = len(seeds)
     return {name + "_spp": spp, name + "_relmse_plain": round(ep / k, 6), name + "_relmse_guided": round(eg / k, 6),
