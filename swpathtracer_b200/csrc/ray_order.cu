@@ -11,12 +11,13 @@
 // per axis, or of the origin when the ray starts inside) above the octant of its direction.  A ray
 // that the traversal's own root test rejects takes no place in the order: the gather writes its miss
 // record, and the traversal runs only over the rays that meet the box (their count is the order's
-// last entry).  The order is a counting sort over the keys without global atomics: every
-// block counts its contiguous share of the rays in a shared-memory histogram (k_order_count), one
-// thread per key turns the per-block counts into each block's first place per key and the key's
-// total (k_order_offsets), and every block scans the totals for the keys' bases and places its rays
-// again from its own counters (k_order_scatter), writing the order and its inverse.  The order of rays within one
-// block's share of a key follows shared-memory atomics and is not fixed; no result depends on it.
+// last entry).  The order is a counting sort over the keys without global atomics: every block
+// counts its contiguous share of the rays in a shared-memory histogram (k_order_count), one thread per
+// key turns the per-block counts into each block's first place per key and the key's total
+// (k_order_offsets), and every block scans the totals for the keys' bases and places its rays again
+// from its own counters (k_order_scatter), writing the order and its inverse.  The order of rays
+// within one block's share of a key follows shared-memory atomics and is not fixed; no result
+// depends on it.
 #include <algorithm>
 
 #include "spt_internal.h"
@@ -255,7 +256,7 @@ __global__ void __launch_bounds__(256) k_order_gather(const spt_hit* __restrict_
 int order_blocks(spt_context* ctx) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-    return sms;   // one 1024-thread block with a 131 KB histogram per SM
+    return sms;   // one 1024-thread block with a 128 KB histogram per SM
 }
 
 }  // namespace
@@ -275,13 +276,13 @@ spt_status order_rays(spt_context* ctx, const spt_scene* sc, const float* d_rays
                                        static_cast<int>(kOrderSmem)));
     const uint32_t n32 = static_cast<uint32_t>(n);
     const int blocks = order_blocks(ctx);
+    if (blocks > 32 * kMaxRowsPerWarp) return fail(ctx, SPT_ERR_UNSUPPORTED, "more SMs than the ray order supports");
     uint32_t* counts = work;
     uint32_t* totals = work + static_cast<size_t>(blocks) * kBins;
     if (stride == 6)
         k_order_count<6><<<blocks, kOrderThreads, kOrderSmem, s>>>(sc->dev, d_rays, n32, keys, counts);
     else
         k_order_count<8><<<blocks, kOrderThreads, kOrderSmem, s>>>(sc->dev, d_rays, n32, keys, counts);
-    if (blocks > 32 * kMaxRowsPerWarp) return fail(ctx, SPT_ERR_UNSUPPORTED, "more SMs than the ray order supports");
     k_order_offsets<<<(kBins + 31) / 32, 1024, 0, s>>>(counts, static_cast<uint32_t>(blocks), totals);
     k_order_scatter<<<blocks, kOrderThreads, kOrderSmem, s>>>(keys, n32, counts, totals, order);
     SPT_CUDA(ctx, cudaGetLastError());
