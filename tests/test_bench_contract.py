@@ -40,3 +40,26 @@ def test_reference_arm_describes_its_cpu_baseline(reference_line):
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["sample"]
     assert cb["value"] == d["value"] and cb["unit"] == d["unit"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_profile_commands_use_flags_bench_accepts():
+    """Every `python bench.py ...` command quoted in profiles/ parses with bench.py's own argument
+    parser, so a profile's recipe keeps running the committed bench as it stands."""
+    import glob
+    import re
+    import shlex
+    cmds = []
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        text = open(path).read().replace("\\\n", " ")
+        for m in re.finditer(r"python bench\.py([^\n>|&`]*)", text):
+            cmds.append((os.path.basename(path), shlex.split(m.group(1))))
+    assert cmds, "no bench commands found in profiles/"
+    for name, argv in cmds:
+        old = sys.argv
+        try:
+            sys.argv = ["bench.py"] + argv
+            bench.args_()
+        except SystemExit as e:
+            pytest.fail("%s: bench.py rejects %s (%s)" % (name, argv, e))
+        finally:
+            sys.argv = old
